@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the isothermal-MHD time step on B200 (one JSON line on rank 0).
+
+Workload (one box per GPU, weak scaling): driven isothermal-MHD turbulence on
+a 512^3 periodic box, FP32 bulk arithmetic, van Leer predictor-corrector with
+characteristic PLM reconstruction, Roe fluxes and constrained transport, two
+passive scalars, rho = 1, cs = 1, B0 = (0.5, 0, 0), initial velocity one
+realisation of the solenoidal OU forcing field (shells 1 <= |k| <= 2) at rms
+Mach 2, forcing kicks on the reference schedule (dt_turb = 0.05), COUR 0.4.
+Synthetic, seeded inputs stand in for the reference's runs.
+
+A step is one call of imhd_step (the reference's copy_velocity +
+vanleer_solve_3d + passive_solve_3d + periodic fill + new dt).  Metric:
+cell-updates/s = N^3 * steps * ranks / max-over-ranks device time.
+
+  python bench.py [--gpus N --steps K --warmup W]      # our CUDA path
+  python bench.py --impl reference                     # CPU restatement of the reference
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+WORKLOAD = ("driven MHD turbulence 512^3 periodic box, FP32 van Leer + PLM-char + Roe + CT, "
+            "2 passive scalars, Mach 2 OU forcing, B0=(0.5,0,0), COUR 0.4")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--riemann", default="roe")
+    ap.add_argument("--precision", type=int, default=32)
+    ap.add_argument("--npass", type=int, default=2)
+    ap.add_argument("--mach", type=float, default=2.0)
+    ap.add_argument("--edot", type=float, default=4.0)
+    ap.add_argument("--cour", type=float, default=0.4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-n", type=int, default=128, help="edge of the CPU sample box")
+    ap.add_argument("--ref-steps", type=int, default=None)
+    ap.add_argument("--seed", type=int, default=20261203)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- distributed
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, init_method="env://", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-i", str(self.idx),
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), power=float(parts[3]),
+                                 hw=parts[5], hwt=parts[6], swt=parts[7], swp=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, name in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"),
+                              ("swt", "sw_thermal_slowdown"), ("swp", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows),
+                "power_w_max": max(r["power"] for r in rows)}
+
+
+# ----------------------------------------------------------------- workload
+def make_initial_state(n, mach, npass, seed):
+    from isothermal_mhd_b200 import forcing
+    f = forcing.OUForcing(n, seed=seed)
+    q, b, p = forcing.turbulent_box(n, mach=mach, b0=(0.5, 0.0, 0.0), npass=npass, seed=seed, forcing=f)
+    f.advance(0.05)
+    delv = f.field(rms=1.0)
+    return q, b, p, delv, f
+
+
+def stage_bytes(esz, npass):
+    """Compulsory HBM bytes per cell of each stage (reads + writes once)."""
+    return {
+        "pred_flux": 3 * 13 * esz,        # per sweep: 7 state fields in, 6 fluxes out
+        "pred_emf": 16 * esz,             # rho, m, B_cc, 6 face EMFs in; 3 corner EMFs out
+        "pred_update": 32 * esz,          # 7 state + 12 fluxes + 3 EMFs in; 10 fields out
+        "corr_flux_x": 13 * esz, "corr_flux_y": 13 * esz, "corr_flux_z": 13 * esz,
+        "corr_emf": 16 * esz,
+        "final_update": 32 * esz,
+        "passive_pred": (4 + 2 * npass) * esz,
+        "passive_corr": (8 + 3 * npass) * esz,
+        "force_sums": 7 * esz, "force_kick": 12 * esz, "finalize": 0,
+    }
+
+
+def run_ours(a, ws, rank, local):
+    import torch
+    from isothermal_mhd_b200 import Box, driver
+
+    dist = init_dist(ws, "nccl")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = a.n
+    q, b, p, delv, f = make_initial_state(n, a.mach, a.npass, a.seed + rank)
+    box = Box(n, precision=a.precision, riemann=a.riemann, npass=a.npass, cour=a.cour, edot=a.edot,
+              dt_turb=0.05, device=local)
+    stream = torch.cuda.current_stream(dev)
+    box.set_stream(stream.cuda_stream)
+    box.upload(q, b, p)
+    box.set_force(delv)
+
+    # the reference driver loop (driver.f90:35-186): dt0 = 1e-15, drive when due
+    state = {"t": 0.0, "dt": 1e-15, "t_turb": 0.05, "drives": 0}
+
+    def one_step():
+        t_old, dt = state["t"], state["dt"]
+        drive = (state["t_turb"] > t_old) and (state["t_turb"] <= t_old + dt)
+        if drive:
+            state["t_turb"] = max(state["t_turb"] + 0.05, t_old + 1e-2 * dt)
+            dt = 0.5 * dt
+        dt_new = box.step(dt, drive)
+        state["t"] = t_old + dt
+        if drive:
+            state["drives"] += 1
+            box.set_force(delv)
+        state["dt"] = dt_new
+
+    for _ in range(a.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    box.profile(True)
+    box.stage_times(reset=True)
+    launches0 = box.launch_count
+    drives0 = state["drives"]
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(a.steps):
+        one_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = box.launch_count - launches0
+    stages = box.stage_times()
+    box.profile(False)
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    cells = n ** 3
+    value = cells * a.steps * ws / (t_max / 1e3)
+
+    # ---- end to end through the C ABI with host buffers: pinned host state in,
+    # K steps (dt in, dt_next out each step), host state out
+    e2e = None
+    if not a.no_e2e:
+        hq = torch.empty(q.shape, dtype=torch.float64, pin_memory=True).numpy()
+        hb = torch.empty(b.shape, dtype=torch.float64, pin_memory=True).numpy()
+        hp = torch.empty(p.shape, dtype=torch.float64, pin_memory=True).numpy()
+        hq[...] = q
+        hb[...] = b
+        hp[...] = p
+        state.update(t=0.0, dt=1e-15, t_turb=0.05)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        box.upload(hq, hb, hp)
+        for _ in range(a.steps):
+            one_step()
+        box.download(hq, hb, hp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        state_bytes = hq.nbytes + hb.nbytes + hp.nbytes
+        e2e = {"value": cells * a.steps * ws / (ems / 1e3), "unit": METRIC,
+               "h2d_bytes_per_step": int(state_bytes / a.steps + 8),
+               "d2h_bytes_per_step": int(state_bytes / a.steps + 12),
+               "ms_total": ems, "includes": "pinned host upload + K imhd_step calls + host download"}
+        del hq, hb, hp
+
+    # ---- roofline of the dominant stage (device time from CUDA events on the launching stream)
+    import json as _json
+    peaks = {}
+    try:
+        peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    esz = 4 if a.precision == 32 else 8
+    sb = stage_bytes(esz, a.npass)
+    per_stage = {}
+    for name, (tot, cnt) in stages.items():
+        if cnt:
+            per_stage[name] = {"ms_per_launch": tot / cnt, "share": None,
+                               "gbs_alg": (sb.get(name, 0) * cells / 1e9) / (tot / cnt / 1e3) if tot > 0 else None}
+    total_stage_ms = sum(v["ms_per_launch"] for v in per_stage.values())
+    for v in per_stage.values():
+        v["share"] = v["ms_per_launch"] / total_stage_ms if total_stage_ms else None
+    dom = max(per_stage, key=lambda k: per_stage[k]["ms_per_launch"])
+    dom_ms = per_stage[dom]["ms_per_launch"]
+    achieved = sb[dom] * cells / 1e9 / (dom_ms / 1e3)
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
+                "algorithmic_bytes_per_launch": sb[dom] * cells, "ms_per_launch": dom_ms}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_reference_sample(a, n_sample=a.ref_n, steps=a.ref_steps or 3, warmup=1)
+
+    box.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == 32 else "f64", "data": "synthetic (seeded OU turbulence)",
+        "config": {"workload": WORKLOAD, "n": n, "precision": a.precision, "riemann": a.riemann,
+                   "recon": "plm-char", "npass": a.npass, "mach": a.mach, "edot": a.edot, "cour": a.cour,
+                   "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (state %.1f GB)" %
+                   ((10 + a.npass) * cells * esz / 1e9), "drive_steps_timed": state["drives"] - drives0},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "stages": per_stage,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    return line
+
+
+# ----------------------------------------------------------------- CPU reference
+def cpu_reference_sample(a, n_sample, steps, warmup):
+    """The CPU restatement of the reference (oracle, FP64, all host threads) on
+    an n_sample^3 box of the same physics; cell-updates/s over `steps` steps."""
+    from oracle.pyoracle import Oracle
+    threads = os.cpu_count() or 1
+    q, b, p, delv, f = make_initial_state(n_sample, a.mach, a.npass, a.seed)
+    o = Oracle(n_sample, riemann=a.riemann, npass=a.npass, nthreads=threads)
+    o.set_state(q, b, p)
+    o.set_force(delv, edot=a.edot, dt_turb=0.05)
+    dt = 1e-15
+    for _ in range(warmup):
+        dt = a.cour * o.dx / o.step(dt)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = a.cour * o.dx / o.step(dt)
+    el = time.perf_counter() - t0
+    o.close()
+    v = n_sample ** 3 * steps / el
+    return {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{n_sample}^3 box of the same physics (FP64), {steps} steps after {warmup} warm-up, "
+                      f"{el:.1f} s; C++ restatement of the reference algorithm (the Fortran build is "
+                      f"unavailable: no Fortran compiler or MPI in the image)"}
+
+
+def run_reference(a, ws, rank):
+    if rank != 0:
+        return None
+    steps = a.ref_steps or max(1, min(a.steps, 10))
+    cpu = cpu_reference_sample(a, n_sample=a.ref_n, steps=steps, warmup=max(1, min(a.warmup, 2)))
+    v = cpu["value"]
+    return {
+        "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": steps, "warmup": a.warmup,
+        "ms_per_step": (a.ref_n ** 3) / v * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded OU turbulence)", "impl": "reference",
+        "config": {"workload": WORKLOAD, "n": a.n, "sample_n": a.ref_n, "riemann": a.riemann, "npass": a.npass,
+                   "parallelism": "host threads"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    a = parse()
+    ws, rank, local = dist_env()
+    if a.impl == "reference":
+        line = run_reference(a, ws, rank)
+    else:
+        line = run_ours(a, ws, rank, local)
+    if line is not None and rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,158 @@
+/*
+ * imhd.h -- C ABI of the B200 isothermal-MHD time-step library (libimhd.so).
+ *
+ * The reference (tsultan16/Isothermal_MHD, 3D_MPI) is a Fortran 90 program
+ * whose hot path is a handful of module procedures acting on module-global
+ * arrays.  This header is the drop-in boundary for that path: a Fortran
+ * driver binds these entry points through ISO_C_BINDING (the binding module
+ * is in INTEGRATION.md), a C/C++ or Python (ctypes) host binds them directly.
+ *
+ * Conventions
+ *  - Every call returns an int status: IMHD_OK (0) or a positive IMHD_E_* code;
+ *    imhd_last_error() returns a message for the calling thread.  Nothing
+ *    throws across this boundary.  (The reference PRINTs and STOPs instead:
+ *    vanleer_mod.f90:131-133, 3328-3331; turb_driver_mod.f90:32-35, 420-425.)
+ *  - Host arrays are borrowed for the duration of the call only.  They use the
+ *    reference's own layout: Fortran column-major, interior cells 1..n per
+ *    axis with `ng` ghost layers on each side, field index slowest.  That is
+ *    q_3d(1-ng:nx+ng,1-ng:ny+ng,1-ng:nz+ng,7), bface_3d(...,3) and
+ *    qpass_3d(1-ngp:nx+ngp,...,npass) of 3D_MPI/src/grid_data_mod.f90:38-43
+ *    (ng = nb = 6 and ngp = nb-2 = 4 there); ng = 0 means unpadded arrays.
+ *  - State lives on the device between calls (one box per handle, one CUDA
+ *    stream per handle).  A handle is not thread safe; use one per host
+ *    thread.
+ *  - Boundaries are periodic (boundary_type = 2, constants_mod.f90:36); the
+ *    ghost zones of the reference become an index wrap inside the kernels.
+ */
+#ifndef IMHD_H
+#define IMHD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IMHD_OK 0
+#define IMHD_E_ARG 1        /* bad argument or configuration */
+#define IMHD_E_CUDA 2       /* CUDA runtime error (no device, launch failure) */
+#define IMHD_E_NOMEM 3      /* device allocation failed */
+#define IMHD_E_PHYSICS 4    /* zero max speed or bad forcing normalisation */
+#define IMHD_E_STATE 5      /* call out of order (e.g. drive without a force field) */
+
+/* Riemann solvers (riemann_solver_type, constants_mod.f90:57) */
+#define IMHD_ROE 1
+#define IMHD_HLLD 2
+#define IMHD_HLLE 3
+
+/* interface reconstruction (piecewise_parabolic, vanleer_mod.f90:83) */
+#define IMHD_PLM 0
+#define IMHD_PPM 1
+
+/* status-word bits reported by imhd_status */
+#define IMHD_S_FLOOR 1u     /* a density fell below 1e-20 and was floored (vanleer_mod.f90:3243-3262) */
+#define IMHD_S_NAN 2u       /* a non-finite max speed was seen */
+#define IMHD_S_ZERO_SPEED 4u/* max speed < 1e-20 (vanleer_mod.f90:3328) */
+#define IMHD_S_FORCE 8u     /* forcing quadratic term <= 1e-20 (turb_driver_mod.f90:420) */
+
+typedef struct imhd_config {
+    int nx, ny, nz;        /* interior cells per axis (constants_mod.f90:9-11) */
+    int precision;         /* 64: FP64 everywhere; 32: FP32 bulk, FP64 reductions */
+    int riemann;           /* IMHD_ROE / IMHD_HLLD / IMHD_HLLE */
+    int recon;             /* IMHD_PLM (IMHD_PPM is reserved) */
+    int npass;             /* passive scalars, 0..8 (constants_mod.f90:63) */
+    double sound_speed;    /* isothermal sound speed (constants_mod.f90:35) */
+    double cour;           /* COUR_def (constants_mod.f90:16) */
+    double edot;           /* kinetic-energy injection rate (constants_mod.f90:44) */
+    double dt_turb;        /* forcing interval (constants_mod.f90:42) */
+    int ng;                /* ghost layers of host q / bface / delv arrays */
+    int ng_pass;           /* ghost layers of host qpass arrays */
+    int device;            /* CUDA device ordinal */
+} imhd_config;
+
+typedef struct imhd_box imhd_box;
+
+/* Fill *cfg with the reference's defaults (64^3, FP64, HLLD, PLM, npass 1,
+ * cs 1, COUR 0.35, Edot 1e-3, dt_turb 0.05, ng 6, ng_pass 4, device 0). */
+void imhd_default_config(imhd_config* cfg);
+
+/* Allocate a box on cfg->device.  Replaces create_grid_arrays
+ * (grid_data_mod.f90:33-67), init_solver_vanleer / allocate_local_variables
+ * (vanleer_mod.f90:127-244) and init_passive_solver (passive_mod.f90:44-111). */
+int imhd_create(const imhd_config* cfg, imhd_box** box);
+
+/* Copy the host state into the box: q_3d, bface_3d (ng ghosts) and qpass_3d
+ * (ng_pass ghosts; may be NULL when npass = 0).  Only interior cells are read.
+ * Replaces the state hand-over after init_state / read_restart
+ * (driver.f90:283-333). */
+int imhd_upload(imhd_box* box, const double* q, const double* bface, const double* qpass);
+
+/* Copy the box state to host arrays in the same layout.  Ghost layers, when
+ * ng > 0, are filled with periodic images, i.e. the arrays read as the
+ * reference's do after boundary_conditions() (boundary_conditions_mod.f90:137-231).
+ * Any pointer may be NULL to skip that array. */
+int imhd_download(imhd_box* box, double* q, double* bface, double* qpass);
+
+/* Set the turbulence forcing field delv(1-ng:nx+ng,...,3), the layout of the
+ * add_random_force dummy argument (turb_driver_mod.f90:398).  Replaces the
+ * hand-over of delv_re produced by generate_rand_force (:197-391). */
+int imhd_set_force(imhd_box* box, const double* delv);
+
+/* One time step of the reference driver loop for one rank: copy_velocity,
+ * vanleer_solve_3d(dt, drive_next) (vanleer_mod.f90:279-426, incl.
+ * get_rho_turb / add_random_force when drive_next != 0), copy_velocity,
+ * passive_solve_3d (passive_mod.f90:118-201), the periodic ghost fill and
+ * compute_new_time_step (driver.f90:55-131, 432-448).  On return *dt_next holds
+ * the new local dt = COUR*dx/cmax with COUR halved after a drive step
+ * (driver.f90:109); the caller applies MIN(t_end - t, dt) (driver.f90:475). */
+int imhd_step(imhd_box* box, double dt, int drive_next, double* dt_next);
+
+/* cmax of the current state alone: get_max_speed_vanleer with smax = 0
+ * (vanleer_mod.f90:3266-3334), used for a first dt without the 1e-15 warm-up. */
+int imhd_max_speed(imhd_box* box, double* cmax);
+
+/* out[0..5] = KE, v_rms^2 sum, momx, momy, momz (compute_KE, driver.f90:518-553)
+ * and the div B sum (compute_divB, driver.f90:492-515), all FP64. */
+int imhd_diagnostics(imhd_box* box, double out[6]);
+
+/* Sticky status word (IMHD_S_* bits) and the count of floored densities;
+ * reset != 0 clears both. */
+int imhd_status(imhd_box* box, unsigned* flags, long long* floor_hits, int reset);
+
+/* smax of the last step (largest interface wave speed, vanleer_mod.f90:2341,
+ * 2962, 3086) and delv_max of the last forcing kick (turb_driver_mod.f90:451). */
+int imhd_wave_speeds(imhd_box* box, double* smax, double* delv_max);
+
+/* Free the box.  Replaces destroy_grid_arrays / destroy_solver_vanleer /
+ * destroy_passive_solver (driver.f90:213-226). */
+void imhd_destroy(imhd_box* box);
+
+/* Message of the last failing call on this thread. */
+const char* imhd_last_error(void);
+
+/* Number of kernel launches issued by this box since creation. */
+long long imhd_launch_count(imhd_box* box);
+
+/* Run the box's device work on the caller's CUDA stream (a cudaStream_t passed
+ * as void*, e.g. the stream of a host framework); NULL restores the box's own
+ * stream.  No reference counterpart (the reference has no device). */
+int imhd_set_stream(imhd_box* box, void* stream);
+
+/* Per-stage CUDA-event timing of imhd_step: enable != 0 switches it on.
+ * No reference counterpart; it plays the role of the reference's MPI_Wtime
+ * brackets around the solve (driver.f90:52, 82-83). */
+int imhd_profile(imhd_box* box, int enable);
+
+/* Accumulated device milliseconds and timed-step counts per stage, in the
+ * launch order of a step: 0 forcing sums, 1 predictor fluxes, 2 predictor
+ * EMF, 3 predictor update, 4-6 corrector fluxes x/y/z, 7 corrector EMF,
+ * 8 final update, 9 forcing kick, 10 passive predictor, 11 passive corrector,
+ * 12 dt finalisation.  n must be IMHD_NSTAGES; reset != 0 clears them. */
+#define IMHD_NSTAGES 13
+int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMHD_H */

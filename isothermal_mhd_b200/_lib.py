@@ -1,0 +1,98 @@
+"""ctypes binding of libimhd.so (the C ABI declared in include/imhd.h).
+
+The library is built in-tree by ``isothermal_mhd_b200.build``.  Loading fails
+loudly when it is missing; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libimhd.so")
+
+IMHD_OK = 0
+ERRORS = {1: "IMHD_E_ARG", 2: "IMHD_E_CUDA", 3: "IMHD_E_NOMEM", 4: "IMHD_E_PHYSICS", 5: "IMHD_E_STATE"}
+S_FLOOR, S_NAN, S_ZERO_SPEED, S_FORCE = 1, 2, 4, 8
+
+# Every symbol declared in include/imhd.h (checked by tests/test_capi_symbols.py).
+EXPORTS = (
+    "imhd_default_config", "imhd_create", "imhd_upload", "imhd_download", "imhd_set_force",
+    "imhd_step", "imhd_max_speed", "imhd_diagnostics", "imhd_status", "imhd_wave_speeds",
+    "imhd_destroy", "imhd_last_error", "imhd_launch_count", "imhd_set_stream", "imhd_profile",
+    "imhd_stage_times",
+)
+NSTAGES = 13
+STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
+          "corr_emf", "final_update", "force_kick", "passive_pred", "passive_corr", "finalize")
+
+
+class ImhdConfig(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("precision", ctypes.c_int), ("riemann", ctypes.c_int), ("recon", ctypes.c_int),
+        ("npass", ctypes.c_int),
+        ("sound_speed", ctypes.c_double), ("cour", ctypes.c_double),
+        ("edot", ctypes.c_double), ("dt_turb", ctypes.c_double),
+        ("ng", ctypes.c_int), ("ng_pass", ctypes.c_int), ("device", ctypes.c_int),
+    ]
+
+
+class ImhdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load libimhd.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m isothermal_mhd_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.imhd_default_config.argtypes = [ctypes.POINTER(ImhdConfig)]
+        L.imhd_default_config.restype = None
+        L.imhd_create.argtypes = [ctypes.POINTER(ImhdConfig), ctypes.POINTER(vp)]
+        L.imhd_create.restype = i
+        L.imhd_upload.argtypes = [vp, dp, dp, dp]
+        L.imhd_upload.restype = i
+        L.imhd_download.argtypes = [vp, dp, dp, dp]
+        L.imhd_download.restype = i
+        L.imhd_set_force.argtypes = [vp, dp]
+        L.imhd_set_force.restype = i
+        L.imhd_step.argtypes = [vp, d, i, dp]
+        L.imhd_step.restype = i
+        L.imhd_max_speed.argtypes = [vp, dp]
+        L.imhd_max_speed.restype = i
+        L.imhd_diagnostics.argtypes = [vp, dp]
+        L.imhd_diagnostics.restype = i
+        L.imhd_status.argtypes = [vp, ctypes.POINTER(ctypes.c_uint), ctypes.POINTER(ctypes.c_longlong), i]
+        L.imhd_status.restype = i
+        L.imhd_wave_speeds.argtypes = [vp, dp, dp]
+        L.imhd_wave_speeds.restype = i
+        L.imhd_destroy.argtypes = [vp]
+        L.imhd_destroy.restype = None
+        L.imhd_last_error.argtypes = []
+        L.imhd_last_error.restype = ctypes.c_char_p
+        L.imhd_launch_count.argtypes = [vp]
+        L.imhd_launch_count.restype = ctypes.c_longlong
+        L.imhd_set_stream.argtypes = [vp, vp]
+        L.imhd_set_stream.restype = i
+        L.imhd_profile.argtypes = [vp, i]
+        L.imhd_profile.restype = i
+        L.imhd_stage_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), i, i]
+        L.imhd_stage_times.restype = i
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != IMHD_OK:
+        raise ImhdError(rc, lib().imhd_last_error().decode(errors="replace"))

@@ -1,0 +1,422 @@
+// imhd_capi.cu -- the extern "C" boundary of libimhd.so (declared in
+// include/imhd.h): box lifetime, host<->device transfer in the reference's
+// array layout, and the per-step call sequence.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/imhd.h"
+#include "imhd_types.cuh"
+
+namespace imhd {
+template <class T> cudaError_t run_step(BoxDev&, int);
+template <class T> cudaError_t run_max_speed(BoxDev&);
+template <class T> cudaError_t run_diag(BoxDev&);
+template <class T> cudaError_t run_from_f64(BoxDev&, const double*, void*);
+template <class T> cudaError_t run_to_f64(BoxDev&, const void*, double*);
+}  // namespace imhd
+
+struct imhd_box {
+    imhd_config cfg;
+    imhd::BoxDev b;
+    size_t esz = 8;
+    double* staging = nullptr;   // N doubles on the device
+    double* hio = nullptr;       // pinned host scalars
+    bool have_force = false;
+    cudaStream_t own_stream = nullptr;
+    double stage_ms[imhd::kStages] = {};
+    long long stage_n[imhd::kStages] = {};
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(IMHD_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool is64(const imhd_box* x) { return x->cfg.precision == 64; }
+
+cudaError_t step_dispatch(imhd_box* x, int drive) {
+    return is64(x) ? imhd::run_step<double>(x->b, drive) : imhd::run_step<float>(x->b, drive);
+}
+
+void* field_ptr(imhd_box* x, void* base, int f) { return (char*)base + (size_t)f * (size_t)x->b.dm.n * x->esz; }
+
+// host field f of a Fortran array a(1-ng:n+ng, ..., nf)
+const double* host_field(const imhd_box* x, const double* h, int f, int ng) {
+    size_t P = (size_t)(x->cfg.nx + 2 * ng) * (x->cfg.ny + 2 * ng) * (x->cfg.nz + 2 * ng);
+    return h + (size_t)f * P;
+}
+
+// Copy the interior of a padded host field into a dense device double array.
+int copy_in_f64(imhd_box* x, const double* hfield, int ng, double* dst) {
+    const imhd_config& c = x->cfg;
+    if (ng == 0) {
+        CK(cudaMemcpyAsync(dst, hfield, (size_t)x->b.dm.n * 8, cudaMemcpyHostToDevice, x->b.st));
+        return IMHD_OK;
+    }
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    p.srcPtr = make_cudaPitchedPtr((void*)hfield, (size_t)(c.nx + 2 * ng) * 8, (size_t)(c.nx + 2 * ng), (size_t)(c.ny + 2 * ng));
+    p.srcPos = make_cudaPos((size_t)ng * 8, (size_t)ng, (size_t)ng);
+    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)c.nx * 8, (size_t)c.nx, (size_t)c.ny);
+    p.dstPos = make_cudaPos(0, 0, 0);
+    p.extent = make_cudaExtent((size_t)c.nx * 8, (size_t)c.ny, (size_t)c.nz);
+    p.kind = cudaMemcpyHostToDevice;
+    CK(cudaMemcpy3DAsync(&p, x->b.st));
+    return IMHD_OK;
+}
+
+int copy_out_f64(imhd_box* x, const double* src, double* hfield, int ng) {
+    const imhd_config& c = x->cfg;
+    if (ng == 0) {
+        CK(cudaMemcpyAsync(hfield, src, (size_t)x->b.dm.n * 8, cudaMemcpyDeviceToHost, x->b.st));
+        return IMHD_OK;
+    }
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    p.srcPtr = make_cudaPitchedPtr((void*)src, (size_t)c.nx * 8, (size_t)c.nx, (size_t)c.ny);
+    p.srcPos = make_cudaPos(0, 0, 0);
+    p.dstPtr = make_cudaPitchedPtr(hfield, (size_t)(c.nx + 2 * ng) * 8, (size_t)(c.nx + 2 * ng), (size_t)(c.ny + 2 * ng));
+    p.dstPos = make_cudaPos((size_t)ng * 8, (size_t)ng, (size_t)ng);
+    p.extent = make_cudaExtent((size_t)c.nx * 8, (size_t)c.ny, (size_t)c.nz);
+    p.kind = cudaMemcpyDeviceToHost;
+    CK(cudaMemcpy3DAsync(&p, x->b.st));
+    return IMHD_OK;
+}
+
+// Upload one host field into device field slot `dst` of precision T.
+int upload_field(imhd_box* x, const double* hfield, int ng, void* dst) {
+    if (is64(x)) return copy_in_f64(x, hfield, ng, (double*)dst);
+    int rc = copy_in_f64(x, hfield, ng, x->staging);
+    if (rc) return rc;
+    CK(imhd::run_from_f64<float>(x->b, x->staging, dst));
+    return IMHD_OK;
+}
+
+int download_field(imhd_box* x, const void* src, double* hfield, int ng) {
+    if (is64(x)) return copy_out_f64(x, (const double*)src, hfield, ng);
+    CK(imhd::run_to_f64<float>(x->b, src, x->staging));
+    return copy_out_f64(x, x->staging, hfield, ng);
+}
+
+// Periodic ghost fill of one padded host field (boundary_conditions_mod.f90:137-231).
+void ghost_fill(const imhd_config& c, double* h, int ng) {
+    if (ng == 0) return;
+    long Px = c.nx + 2 * ng, Py = c.ny + 2 * ng, Pz = c.nz + 2 * ng;
+    auto wrap = [](long i, long n) { i %= n; return i < 0 ? i + n : i; };
+    for (long k = 0; k < Pz; ++k) {
+        long kk = wrap(k - ng, c.nz) + ng;
+        bool kin = (k >= ng && k < ng + c.nz);
+        for (long j = 0; j < Py; ++j) {
+            long jj = wrap(j - ng, c.ny) + ng;
+            bool jin = (j >= ng && j < ng + c.ny);
+            for (long i = 0; i < Px; ++i) {
+                bool iin = (i >= ng && i < ng + c.nx);
+                if (iin && jin && kin) continue;
+                long ii = wrap(i - ng, c.nx) + ng;
+                h[i + Px * (j + Py * k)] = h[ii + Px * (jj + Py * kk)];
+            }
+        }
+    }
+}
+
+int sync_and_check(imhd_box* x) {
+    CK(cudaStreamSynchronize(x->b.st));
+    CK(cudaGetLastError());
+    return IMHD_OK;
+}
+
+// Fold the events of the last step into the per-stage accumulators.
+int accumulate_stage_times(imhd_box* x) {
+    imhd::BoxDev& b = x->b;
+    if (!b.prof) return IMHD_OK;
+    for (int s = 0; s < imhd::kStages; ++s) {
+        if (!(b.prof_mask & (1u << s))) continue;
+        int nxt = s + 1;
+        while (nxt < imhd::kStages && !(b.prof_mask & (1u << nxt))) ++nxt;
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, b.ev[s], b.ev[nxt]));
+        x->stage_ms[s] += ms;
+        x->stage_n[s] += 1;
+    }
+    return IMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void imhd_default_config(imhd_config* c) {
+    std::memset(c, 0, sizeof(*c));
+    c->nx = c->ny = c->nz = 64;
+    c->precision = 64;
+    c->riemann = IMHD_HLLD;
+    c->recon = IMHD_PLM;
+    c->npass = 1;
+    c->sound_speed = 1.0;
+    c->cour = 0.35;
+    c->edot = 1.0e-3;
+    c->dt_turb = 0.05;
+    c->ng = 6;
+    c->ng_pass = 4;
+    c->device = 0;
+}
+
+const char* imhd_last_error(void) { return g_err.c_str(); }
+
+int imhd_create(const imhd_config* cfg, imhd_box** out) {
+    if (!cfg || !out) return fail(IMHD_E_ARG, "null argument");
+    *out = nullptr;
+    const imhd_config& c = *cfg;
+    if (c.nx < 4 || c.ny < 4 || c.nz < 4) return fail(IMHD_E_ARG, "every edge needs at least 4 cells");
+    if ((double)c.nx * c.ny * c.nz >= 2147483647.0) return fail(IMHD_E_ARG, "box too large (nx*ny*nz must be < 2^31)");
+    if (c.precision != 32 && c.precision != 64) return fail(IMHD_E_ARG, "precision must be 32 or 64");
+    if (c.riemann < 1 || c.riemann > 3) return fail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
+    if (c.recon != IMHD_PLM) return fail(IMHD_E_ARG, "only IMHD_PLM reconstruction is implemented");
+    if (c.npass < 0 || c.npass > imhd::kMaxPass) return fail(IMHD_E_ARG, "npass must be in 0..8");
+    if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return fail(IMHD_E_ARG, "sound_speed and cour must be positive");
+    if (c.ng < 0 || c.ng_pass < 0) return fail(IMHD_E_ARG, "ghost widths must be >= 0");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (c.device < 0 || c.device >= ndev) return fail(IMHD_E_ARG, "no such CUDA device");
+    CK(cudaSetDevice(c.device));
+
+    imhd_box* x = new imhd_box();
+    x->cfg = c;
+    x->esz = c.precision == 64 ? 8 : 4;
+    imhd::BoxDev& b = x->b;
+    b.dm.nx = c.nx; b.dm.ny = c.ny; b.dm.nz = c.nz; b.dm.n = c.nx * c.ny * c.nz;
+    b.riemann = c.riemann;
+    b.npass = c.npass;
+    b.cs = c.sound_speed;
+    int nmax = c.nx > c.ny ? c.nx : c.ny;
+    nmax = nmax > c.nz ? nmax : c.nz;
+    b.dx = 1.0 / (double)nmax;                  // vanleer_mod.f90:177, driver.f90:254
+    b.cour = c.cour;
+    b.edot = c.edot;
+    b.dt_turb = c.dt_turb;
+    int pmax = c.ny * c.nz;
+    if (c.nx * c.nz > pmax) pmax = c.nx * c.nz;
+    if (c.nx * c.ny > pmax) pmax = c.nx * c.ny;
+    b.plane_stride = pmax;
+    b.nred = 1024;
+    size_t N = (size_t)b.dm.n;
+    size_t nf = 10 + (size_t)c.npass;
+    auto alloc = [&](void** p, size_t bytes) -> bool { return cudaMalloc(p, bytes) == cudaSuccess; };
+    bool ok = cudaStreamCreateWithFlags(&b.st, cudaStreamNonBlocking) == cudaSuccess;
+    x->own_stream = b.st;
+    ok = ok && alloc(&b.A, nf * N * x->esz) && alloc(&b.B, nf * N * x->esz) && alloc(&b.F, 18 * N * x->esz) &&
+         alloc(&b.E, 3 * N * x->esz) && alloc((void**)&b.partials, (size_t)b.nred * 6 * 8) &&
+         alloc((void**)&b.sc, sizeof(imhd::Scalars)) && alloc((void**)&x->staging, N * 8);
+    if (ok && c.npass > 0) ok = alloc(&b.SH, (size_t)c.npass * N * x->esz) && alloc(&b.mbnd, 6 * (size_t)pmax * x->esz);
+    if (ok) ok = cudaMallocHost((void**)&x->hio, 64 * sizeof(double)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        imhd_destroy(x);
+        return fail(IMHD_E_NOMEM, "device allocation failed");
+    }
+    cudaMemsetAsync(b.sc, 0, sizeof(imhd::Scalars), b.st);
+    cudaMemsetAsync(b.A, 0, nf * N * x->esz, b.st);
+    cudaMemsetAsync(b.B, 0, nf * N * x->esz, b.st);
+    int rc = sync_and_check(x);
+    if (rc) { imhd_destroy(x); return rc; }
+    *out = x;
+    return IMHD_OK;
+}
+
+void imhd_destroy(imhd_box* x) {
+    if (!x) return;
+    cudaSetDevice(x->cfg.device);
+    if (x->b.st) cudaStreamSynchronize(x->b.st);
+    if (x->own_stream) cudaStreamSynchronize(x->own_stream);
+    void* ptrs[] = {x->b.A, x->b.B, x->b.F, x->b.E, x->b.SH, x->b.delv, x->b.mbnd, x->b.partials, x->b.sc, x->staging};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (x->hio) cudaFreeHost(x->hio);
+    for (int s = 0; s <= imhd::kStages; ++s)
+        if (x->b.ev[s]) cudaEventDestroy(x->b.ev[s]);
+    if (x->own_stream) cudaStreamDestroy(x->own_stream);
+    delete x;
+}
+
+int imhd_upload(imhd_box* x, const double* q, const double* bface, const double* qpass) {
+    if (!x || !q || !bface) return fail(IMHD_E_ARG, "null argument");
+    if (x->cfg.npass > 0 && !qpass) return fail(IMHD_E_ARG, "qpass is NULL but npass > 0");
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    for (int f = 0; f < 7; ++f)
+        if ((rc = upload_field(x, host_field(x, q, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.A, f)))) return rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = upload_field(x, host_field(x, bface, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.A, 7 + f)))) return rc;
+    for (int f = 0; f < x->cfg.npass; ++f)
+        if ((rc = upload_field(x, host_field(x, qpass, f, x->cfg.ng_pass), x->cfg.ng_pass, field_ptr(x, x->b.A, 10 + f))))
+            return rc;
+    return sync_and_check(x);
+}
+
+int imhd_download(imhd_box* x, double* q, double* bface, double* qpass) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    const imhd_config& c = x->cfg;
+    // the transfers of one field reuse the staging buffer, so each field is
+    // completed (stream-ordered) before the next conversion overwrites it
+    if (q)
+        for (int f = 0; f < 7; ++f) {
+            if ((rc = download_field(x, field_ptr(x, x->b.A, f), (double*)host_field(x, q, f, c.ng), c.ng))) return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (bface)
+        for (int f = 0; f < 3; ++f) {
+            if ((rc = download_field(x, field_ptr(x, x->b.A, 7 + f), (double*)host_field(x, bface, f, c.ng), c.ng))) return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (qpass && c.npass > 0)
+        for (int f = 0; f < c.npass; ++f) {
+            if ((rc = download_field(x, field_ptr(x, x->b.A, 10 + f), (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass)))
+                return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (q) for (int f = 0; f < 7; ++f) ghost_fill(c, (double*)host_field(x, q, f, c.ng), c.ng);
+    if (bface) for (int f = 0; f < 3; ++f) ghost_fill(c, (double*)host_field(x, bface, f, c.ng), c.ng);
+    if (qpass) for (int f = 0; f < c.npass; ++f) ghost_fill(c, (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass);
+    return IMHD_OK;
+}
+
+int imhd_set_force(imhd_box* x, const double* delv) {
+    if (!x || !delv) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    if (!x->b.delv) {
+        if (cudaMalloc(&x->b.delv, 3 * (size_t)x->b.dm.n * x->esz) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(IMHD_E_NOMEM, "device allocation of the force field failed");
+        }
+    }
+    int rc;
+    for (int f = 0; f < 3; ++f) {
+        if ((rc = upload_field(x, host_field(x, delv, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.delv, f)))) return rc;
+        if ((rc = sync_and_check(x))) return rc;
+    }
+    x->have_force = true;
+    return IMHD_OK;
+}
+
+int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    if (!(dt > 0.0)) return fail(IMHD_E_ARG, "dt must be positive");
+    if (drive_next && !x->have_force) return fail(IMHD_E_STATE, "drive step requested before imhd_set_force");
+    CK(cudaSetDevice(x->cfg.device));
+    x->hio[0] = dt;
+    CK(cudaMemcpyAsync(&x->b.sc->dt, x->hio, sizeof(double), cudaMemcpyHostToDevice, x->b.st));
+    CK(step_dispatch(x, drive_next ? 1 : 0));
+    std::swap(x->b.A, x->b.B);
+    CK(cudaMemcpyAsync(x->hio + 1, &x->b.sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync((unsigned*)(x->hio + 2), &x->b.sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    if ((rc = accumulate_stage_times(x))) return rc;
+    if (dt_next) *dt_next = x->hio[1];
+    unsigned st = *(unsigned*)(x->hio + 2);
+    if (st & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
+    if (st & IMHD_S_FORCE) return fail(IMHD_E_PHYSICS, "bad value in turbulence driver energy normalisation");
+    return IMHD_OK;
+}
+
+int imhd_max_speed(imhd_box* x, double* cmax) {
+    if (!x || !cmax) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    CK(is64(x) ? imhd::run_max_speed<double>(x->b) : imhd::run_max_speed<float>(x->b));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(x->hio + 3, &x->b.sc->cfl0_bits, 8, cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    std::memcpy(&bits, x->hio + 3, 8);
+    std::memcpy(cmax, &bits, 8);
+    return IMHD_OK;
+}
+
+int imhd_diagnostics(imhd_box* x, double out[6]) {
+    if (!x || !out) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    CK(is64(x) ? imhd::run_diag<double>(x->b) : imhd::run_diag<float>(x->b));
+    CK(cudaMemcpyAsync(x->hio + 8, &x->b.sc->diag[0], 6 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    for (int q = 0; q < 6; ++q) out[q] = x->hio[8 + q];
+    return IMHD_OK;
+}
+
+int imhd_status(imhd_box* x, unsigned* flags, long long* floor_hits, int reset) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    imhd::Scalars s;
+    CK(cudaMemcpyAsync(&s, x->b.sc, sizeof(s), cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    unsigned f = s.status;
+    if (s.floor_hits) f |= IMHD_S_FLOOR;
+    if (flags) *flags = f;
+    if (floor_hits) *floor_hits = (long long)s.floor_hits;
+    if (reset) {
+        CK(cudaMemsetAsync(&x->b.sc->status, 0, sizeof(unsigned), x->b.st));
+        CK(cudaMemsetAsync(&x->b.sc->floor_hits, 0, sizeof(unsigned long long), x->b.st));
+        return sync_and_check(x);
+    }
+    return IMHD_OK;
+}
+
+int imhd_wave_speeds(imhd_box* x, double* smax, double* delv_max) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    CK(cudaMemcpyAsync(x->hio + 16, &x->b.sc->smax_last, 2 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    if (smax) *smax = x->hio[16];
+    if (delv_max) *delv_max = x->hio[17];
+    return IMHD_OK;
+}
+
+long long imhd_launch_count(imhd_box* x) { return x ? x->b.launches : 0; }
+
+int imhd_set_stream(imhd_box* x, void* stream) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    CK(cudaStreamSynchronize(x->b.st));
+    x->b.st = stream ? (cudaStream_t)stream : x->own_stream;
+    return IMHD_OK;
+}
+
+int imhd_profile(imhd_box* x, int enable) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    if (enable && !x->b.ev[0])
+        for (int s = 0; s <= imhd::kStages; ++s) CK(cudaEventCreate(&x->b.ev[s]));
+    x->b.prof = enable != 0;
+    return IMHD_OK;
+}
+
+int imhd_stage_times(imhd_box* x, double* ms, long long* count, int n, int reset) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    if (n != imhd::kStages) return fail(IMHD_E_ARG, "n must be IMHD_NSTAGES");
+    for (int s = 0; s < n; ++s) {
+        if (ms) ms[s] = x->stage_ms[s];
+        if (count) count[s] = x->stage_n[s];
+        if (reset) { x->stage_ms[s] = 0.0; x->stage_n[s] = 0; }
+    }
+    return IMHD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,746 @@
+// imhd_kernels.cuh -- CUDA kernels of one isothermal-MHD van Leer + CT step on
+// a periodic box, templated on the arithmetic type (float / double).
+//
+// Data layout in HBM (one box): structure of arrays, x fastest, no ghost
+// cells; the reference's nb-wide ghost zones (grid_data_mod.f90:38-43) become
+// an index wrap.  A state buffer holds 10 + npass fields of N = nx*ny*nz:
+//   0 rho, 1..3 momentum, 4..6 cell-centred B, 7..9 face B (x at i+1/2,
+//   y at j+1/2, z at k+1/2, as bface_3d), 10.. passive scalars.
+// Flux buffer: 18 fields, F[6*D + c] with c in the rotated order
+// (rho, m_n, m_t1, m_t2, B_t1, B_t2) of sweep D, stored at the cell left of
+// the face.  Corner EMF buffer: Ex(i,j+1/2,k+1/2), Ey(i+1/2,j,k+1/2),
+// Ez(i+1/2,j+1/2,k), as emf_corner (vanleer_mod.f90:1868-1882).
+//
+// Because periodic ghost cells are exact images of interior cells, every
+// flux, EMF and update the reference computes in its padded arrays is either
+// computed here for the interior cell it images or is not needed by interior
+// cells; interior results and the smax reduction are therefore identical.
+// One exception is replicated explicitly: on drive steps the reference
+// applies the forcing kick to interior cells only (turb_driver_mod.f90:437-453)
+// and then builds the passive-scalar advection velocity from its ghost cells
+// (passive_mod.f90:227-239), so the face velocity at the global boundary sees
+// the unforced momentum of the ghost side (k_passive_corr below).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "imhd_physics.cuh"
+#include "imhd_types.cuh"
+
+namespace imhd {
+
+__device__ __forceinline__ int wrap_up(int i, int n) { return (i + 1 == n) ? 0 : i + 1; }
+__device__ __forceinline__ int wrap_dn(int i, int n) { return (i == 0) ? n - 1 : i - 1; }
+__device__ __forceinline__ int wrap_any(int i, int n) { i %= n; return i < 0 ? i + n : i; }
+
+template <class T>
+__device__ __forceinline__ const T* fld(const T* S, int f, int n) { return S + (size_t)f * (size_t)n; }
+template <class T>
+__device__ __forceinline__ T* fld(T* S, int f, int n) { return S + (size_t)f * (size_t)n; }
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = vmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// all 32 lanes of the warp must call this
+__device__ __forceinline__ void warp_atomic_max(unsigned long long* addr, double v) {
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0 && !(v <= 0.0))   // NaN bits exceed every finite value
+        atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// rotated field indices of sweep D (vanleer_mod.f90:443-461, 605-630, 784-806)
+template <int D> struct Rot {
+    static constexpr int MN = 1 + D, MT1 = 1 + (D + 1) % 3, MT2 = 1 + (D + 2) % 3;
+    static constexpr int BT1 = 4 + (D + 1) % 3, BT2 = 4 + (D + 2) % 3, BN = 7 + D;
+};
+
+// ============================================================ predictor flux
+// First-order interface fluxes (compute_{x,y,z}fluxes_3d with
+// corrector_stage = .FALSE., vanleer_mod.f90:441-478): left/right states are
+// the cell values, the normal field the face value.
+template <class T, int SOLVER, int D>
+__global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
+                                                   T asqr, unsigned long long* smax_bits) {
+    using R = Rot<D>;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    bool valid = i < dm.nx;
+    T smax = T(0);
+    if (valid) {
+        int c = i + dm.nx * (j + dm.ny * k);
+        int cn;
+        if (D == 0) cn = wrap_up(i, dm.nx) + dm.nx * (j + dm.ny * k);
+        else if (D == 1) cn = i + dm.nx * (wrap_up(j, dm.ny) + dm.ny * k);
+        else cn = i + dm.nx * (j + dm.ny * wrap_up(k, dm.nz));
+        T uL[7], uR[7];
+        uL[0] = fld(S, 0, dm.n)[c]; uL[1] = fld(S, R::MN, dm.n)[c]; uL[2] = fld(S, R::MT1, dm.n)[c];
+        uL[3] = fld(S, R::MT2, dm.n)[c]; uL[4] = fld(S, R::BN, dm.n)[c];
+        uL[5] = fld(S, R::BT1, dm.n)[c]; uL[6] = fld(S, R::BT2, dm.n)[c];
+        uR[0] = fld(S, 0, dm.n)[cn]; uR[1] = fld(S, R::MN, dm.n)[cn]; uR[2] = fld(S, R::MT1, dm.n)[cn];
+        uR[3] = fld(S, R::MT2, dm.n)[cn]; uR[4] = uL[4];
+        uR[5] = fld(S, R::BT1, dm.n)[cn]; uR[6] = fld(S, R::BT2, dm.n)[cn];
+        T Fo[7];
+        riemann<SOLVER>(uL, uR, cs, asqr, Fo, smax);
+        T* Fd = F + (size_t)(6 * D) * dm.n;
+        Fd[c] = Fo[0];
+        Fd[(size_t)dm.n + c] = Fo[1];
+        Fd[2 * (size_t)dm.n + c] = Fo[2];
+        Fd[3 * (size_t)dm.n + c] = Fo[3];
+        Fd[4 * (size_t)dm.n + c] = Fo[5];
+        Fd[5 * (size_t)dm.n + c] = Fo[6];
+    }
+    warp_atomic_max(smax_bits, (double)smax);
+}
+
+// ============================================================ corrector flux
+// Primitive variables of a cell in the rotated frame of sweep D
+// (vanleer_mod.f90:483-496): rho, v_n, v_t1, v_t2, B_t1, B_t2.
+template <class T, int D>
+__device__ __forceinline__ void load_prim(const T* __restrict__ S, int n, int c, T* w, T& bn) {
+    using R = Rot<D>;
+    T rho = fld(S, 0, n)[c];
+    T irho = T(1) / rho;
+    w[0] = rho;
+    w[1] = fld(S, R::MN, n)[c] * irho;
+    w[2] = fld(S, R::MT1, n)[c] * irho;
+    w[3] = fld(S, R::MT2, n)[c] * irho;
+    w[4] = fld(S, R::BT1, n)[c];
+    w[5] = fld(S, R::BT2, n)[c];
+    bn = fld(S, R::BN, n)[c];
+}
+
+template <class T>
+__device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int c, const T* Fo) {
+    T* Fd = F + (size_t)(6 * D) * n;
+    Fd[c] = Fo[0];
+    Fd[(size_t)n + c] = Fo[1];
+    Fd[2 * (size_t)n + c] = Fo[2];
+    Fd[3 * (size_t)n + c] = Fo[3];
+    Fd[4 * (size_t)n + c] = Fo[5];
+    Fd[5 * (size_t)n + c] = Fo[6];
+}
+
+// Sweeps along y (D=1) and z (D=2): one thread per (x, transverse) column
+// marches along the sweep direction over a segment of faces, keeping the
+// primitive window w(a-1..a+2) and the slopes delw(a), delw(a+1) in
+// registers.  Loads stay coalesced along x.
+template <class T, int SOLVER, int D>
+__global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S, T* __restrict__ F, Dims dm,
+                                                         int seg, T cs, T asqr, unsigned long long* smax_bits) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int o = blockIdx.y;                         // k for D=1, j for D=2
+    int a0 = blockIdx.z * seg;
+    int na = (D == 1) ? dm.ny : dm.nz;
+    int a1 = min(a0 + seg, na);
+    bool valid = i < dm.nx;
+    T smax = T(0);
+    if (valid) {
+        int stride = (D == 1) ? dm.nx : dm.nx * dm.ny;
+        int base = (D == 1) ? i + dm.nx * dm.ny * o : i + dm.nx * o;
+        T wa[6], wb_[6], wc[6], wd[6];   // w(a-1), w(a), w(a+1), w(a+2)
+        T bnA, bnB, tmpbn;
+        T dA[6], dB[6];                  // delw(a), delw(a+1)
+        load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wa, tmpbn);
+        load_prim<T, D>(S, dm.n, base + a0 * stride, wb_, bnA);
+        load_prim<T, D>(S, dm.n, base + wrap_up(a0, na) * stride, wc, bnB);
+        plm_char_slope(wa, wb_, wc, bnA, cs, asqr, dA);
+        for (int a = a0; a < a1; ++a) {
+            int ap1 = wrap_up(a, na);
+            int ap2 = wrap_up(ap1, na);
+            T bnC;
+            load_prim<T, D>(S, dm.n, base + ap2 * stride, wd, bnC);
+            plm_char_slope(wb_, wc, wd, bnB, cs, asqr, dB);
+            T qL[7], qR[7], Fo[7];
+            plm_left_state(wb_, dA, bnA, qL);
+            plm_right_state(wc, dB, bnA, qR);
+            riemann<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+            store_flux(F, D, dm.n, base + a * stride, Fo);
+#pragma unroll
+            for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
+            bnA = bnB; bnB = bnC;
+        }
+    }
+    warp_atomic_max(smax_bits, (double)smax);
+}
+
+// Sweep along x: a block covers TX faces of one (j,k) row; primitives of the
+// TX+3 cells and the TX+1 slopes are staged in shared memory.
+template <class T, int SOLVER, int TX>
+__global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
+                                                    T asqr, unsigned long long* smax_bits) {
+    __shared__ T sw[6][TX + 3];
+    __shared__ T sbn[TX + 3];
+    __shared__ T sd[6][TX + 1];
+    int i0 = blockIdx.x * TX;
+    int j = blockIdx.y, k = blockIdx.z;
+    int row = dm.nx * (j + dm.ny * k);
+    for (int t = threadIdx.x; t < TX + 3; t += TX) {
+        int ii = wrap_any(i0 - 1 + t, dm.nx);
+        T w[6], bn;
+        load_prim<T, 0>(S, dm.n, row + ii, w, bn);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) sw[m][t] = w[m];
+        sbn[t] = bn;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < TX + 1; t += TX) {
+        T wm[6], w0[6], wp[6], d[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) { wm[m] = sw[m][t]; w0[m] = sw[m][t + 1]; wp[m] = sw[m][t + 2]; }
+        plm_char_slope(wm, w0, wp, sbn[t + 1], cs, asqr, d);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) sd[m][t] = d[m];
+    }
+    __syncthreads();
+    int t = threadIdx.x;
+    int i = i0 + t;
+    T smax = T(0);
+    if (i < dm.nx) {
+        T wl[6], wr[6], dl[6], dr[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) { wl[m] = sw[m][t + 1]; wr[m] = sw[m][t + 2]; dl[m] = sd[m][t]; dr[m] = sd[m][t + 1]; }
+        T bn = sbn[t + 1];
+        T qL[7], qR[7], Fo[7];
+        plm_left_state(wl, dl, bn, qL);
+        plm_right_state(wr, dr, bn, qR);
+        riemann<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+        store_flux(F, 0, dm.n, row + i, Fo);
+    }
+    warp_atomic_max(smax_bits, (double)smax);
+}
+
+// ============================================================ corner EMF
+// compute_cell_center_emf_3d (vanleer_mod.f90:1823-1862) evaluated on the fly
+// and compute_cell_corner_emf_3d (:1884-2076).  Face EMFs come from the flux
+// of the transverse field (:554-555, 726-727, 903-904).
+template <class T>
+__device__ __forceinline__ T ecc(const T* __restrict__ S, int n, int c, int comp) {
+    T irho = T(1) / fld(S, 0, n)[c];
+    T mx = fld(S, 1, n)[c], my = fld(S, 2, n)[c], mz = fld(S, 3, n)[c];
+    T bx = fld(S, 4, n)[c], by = fld(S, 5, n)[c], bz = fld(S, 6, n)[c];
+    if (comp == 0) return (by * mz - bz * my) * irho;
+    if (comp == 1) return (bz * mx - bx * mz) * irho;
+    return (bx * my - by * mx) * irho;
+}
+template <class T>
+__device__ __forceinline__ T face_v(const T* __restrict__ S, int n, int c, int cn, int comp) {
+    return T(0.5) * (fld(S, 1 + comp, n)[c] / fld(S, 0, n)[c] + fld(S, 1 + comp, n)[cn] / fld(S, 0, n)[cn]);
+}
+template <class T>
+__device__ __forceinline__ void upwind_pair(T v, T L14, T R14, T L34, T R34, T& o14, T& o34) {
+    if (v > T(kZERO)) { o14 = L14; o34 = L34; }
+    else if (v < -T(kZERO)) { o14 = R14; o34 = R34; }
+    else { o14 = T(0.5) * (L14 + R14); o34 = T(0.5) * (L34 + R34); }
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_corner_emf(const T* __restrict__ S, const T* __restrict__ F,
+                                                    T* __restrict__ E, Dims dm) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i >= dm.nx) return;
+    const int n = dm.n;
+    int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny), kp = wrap_up(k, dm.nz);
+    auto C = [&](int a, int b, int c) { return a + dm.nx * (b + dm.ny * c); };
+    int c000 = C(i, j, k), c100 = C(ip, j, k), c010 = C(i, jp, k), c001 = C(i, j, kp);
+    int c110 = C(ip, jp, k), c101 = C(ip, j, kp), c011 = C(i, jp, kp);
+    // face EMFs: E_{t2} = -F_bt1, E_{t1} = F_bt2 of sweep D
+    const T* Fx_bt1 = F + (size_t)4 * n;    // x sweep: -Ez at x-face
+    const T* Fx_bt2 = F + (size_t)5 * n;    //           Ey at x-face
+    const T* Fy_bt1 = F + (size_t)10 * n;   // y sweep: -Ex at y-face
+    const T* Fy_bt2 = F + (size_t)11 * n;   //           Ez at y-face
+    const T* Fz_bt1 = F + (size_t)16 * n;   // z sweep: -Ey at z-face
+    const T* Fz_bt2 = F + (size_t)17 * n;   //           Ex at z-face
+    T vx = face_v(S, n, c000, c100, 0);
+    T vy = face_v(S, n, c000, c010, 1);
+    T vz = face_v(S, n, c000, c001, 2);
+    // Ez at (i+1/2, j+1/2, k)
+    {
+        T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
+        T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
+        T E33_000 = ecc(S, n, c000, 2), E33_100 = ecc(S, n, c100, 2), E33_010 = ecc(S, n, c010, 2), E33_110 = ecc(S, n, c110, 2);
+        T dyL14 = T(2) * (E32_000 - E33_000);
+        T dyR14 = T(2) * (E32_100 - E33_100);
+        T dyL34 = T(2) * (E33_010 - E32_000);
+        T dyR34 = T(2) * (E33_110 - E32_100);
+        T dy1214, dy1234;
+        upwind_pair(vx, dyL14, dyR14, dyL34, dyR34, dy1214, dy1234);
+        T dxL14 = T(2) * (E31_000 - E33_000);
+        T dxR14 = T(2) * (E31_010 - E33_010);
+        T dxL34 = T(2) * (E33_100 - E31_000);
+        T dxR34 = T(2) * (E33_110 - E31_010);
+        T dx1412, dx3412;
+        upwind_pair(vy, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+        E[(size_t)2 * n + c000] = T(0.25) * (E31_000 + E31_010 + E32_000 + E32_100) +
+                                  T(0.125) * ((dy1214 - dy1234) + (dx1412 - dx3412));
+    }
+    // Ey at (i+1/2, j, k+1/2)
+    {
+        T E21_000 = Fx_bt2[c000], E21_001 = Fx_bt2[c001];
+        T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
+        T E23_000 = ecc(S, n, c000, 1), E23_100 = ecc(S, n, c100, 1), E23_001 = ecc(S, n, c001, 1), E23_101 = ecc(S, n, c101, 1);
+        T dzL14 = T(2) * (E22_000 - E23_000);
+        T dzR14 = T(2) * (E22_100 - E23_100);
+        T dzL34 = T(2) * (E23_001 - E22_000);
+        T dzR34 = T(2) * (E23_101 - E22_100);
+        T dz1214, dz1234;
+        upwind_pair(vx, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+        T dxL14 = T(2) * (E21_000 - E23_000);
+        T dxR14 = T(2) * (E21_001 - E23_001);
+        T dxL34 = T(2) * (E23_100 - E21_000);
+        T dxR34 = T(2) * (E23_101 - E21_001);
+        T dx1412, dx3412;
+        upwind_pair(vz, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+        E[(size_t)1 * n + c000] = T(0.25) * (E21_000 + E21_001 + E22_000 + E22_100) +
+                                  T(0.125) * ((dz1214 - dz1234) + (dx1412 - dx3412));
+    }
+    // Ex at (i, j+1/2, k+1/2)
+    {
+        T E11_000 = -Fy_bt1[c000], E11_001 = -Fy_bt1[c001];
+        T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
+        T E13_000 = ecc(S, n, c000, 0), E13_010 = ecc(S, n, c010, 0), E13_001 = ecc(S, n, c001, 0), E13_011 = ecc(S, n, c011, 0);
+        T dzL14 = T(2) * (E12_000 - E13_000);
+        T dzR14 = T(2) * (E12_010 - E13_010);
+        T dzL34 = T(2) * (E13_001 - E12_000);
+        T dzR34 = T(2) * (E13_011 - E12_010);
+        T dz1214, dz1234;
+        upwind_pair(vy, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+        T dyL14 = T(2) * (E11_000 - E13_000);
+        T dyR14 = T(2) * (E11_001 - E13_001);
+        T dyL34 = T(2) * (E13_010 - E11_000);
+        T dyR34 = T(2) * (E13_011 - E11_001);
+        T dy1412, dy3412;
+        upwind_pair(vz, dyL14, dyR14, dyL34, dyR34, dy1412, dy3412);
+        E[c000] = T(0.25) * (E11_000 + E11_001 + E12_000 + E12_010) +
+                  T(0.125) * ((dz1214 - dz1234) + (dy1412 - dy3412));
+    }
+}
+
+// ============================================================ update
+// update_hydro_state_3d + final_check_unphysical (vanleer_mod.f90:2080-2207,
+// 3243-3262) and update_CT_3d with the cell-centre average (:2211-2259).
+// Reads the step-start state S0 and writes Sout.  With do_cfl the fast-speed
+// maximum of the new state (get_max_speed_vanleer :3281-3318) is folded in.
+template <class T>
+__device__ __forceinline__ T ct_bx(const T* __restrict__ S0, const T* __restrict__ E, int n, T dtdx, int c, int cym,
+                                   int czm) {
+    return fld(S0, 7, n)[c] - dtdx * ((E[2 * (size_t)n + c] - E[2 * (size_t)n + cym]) - (E[(size_t)n + c] - E[(size_t)n + czm]));
+}
+template <class T>
+__device__ __forceinline__ T ct_by(const T* __restrict__ S0, const T* __restrict__ E, int n, T dtdx, int c, int czm,
+                                   int cxm) {
+    return fld(S0, 8, n)[c] - dtdx * ((E[c] - E[czm]) - (E[2 * (size_t)n + c] - E[2 * (size_t)n + cxm]));
+}
+template <class T>
+__device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict__ E, int n, T dtdx, int c, int cxm,
+                                   int cym) {
+    return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_update(const T* __restrict__ S0, const T* __restrict__ F,
+                                                const T* __restrict__ E, T* __restrict__ Sout, Dims dm,
+                                                const Scalars* __restrict__ sc, double dt_scale, double dx, T asqr,
+                                                int do_cfl, unsigned long long* cmax_bits,
+                                                unsigned long long* floor_hits, unsigned int* status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    bool valid = i < dm.nx;
+    double cmax = 0.0;
+    if (valid) {
+        const int n = dm.n;
+        T dtdx = (T)(dt_scale * sc->dt / dx);
+        int im = wrap_dn(i, dm.nx), jm = wrap_dn(j, dm.ny), km = wrap_dn(k, dm.nz);
+        auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
+        int c = C(i, j, k), cxm = C(im, j, k), cym = C(i, jm, k), czm = C(i, j, km);
+        T out[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            // flux component of xyz variable v in sweep D: rho -> 0; momentum X -> 1 + (X - D) mod 3
+            int fx = (v == 0) ? 0 : 1 + (v - 1 + 3) % 3;
+            int fy = (v == 0) ? 0 : 1 + (v - 1 - 1 + 3) % 3;
+            int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
+            const T* Fx = F + (size_t)(0 + fx) * n;
+            const T* Fy = F + (size_t)(6 + fy) * n;
+            const T* Fz = F + (size_t)(12 + fz) * n;
+            out[v] = fld(S0, v, n)[c] - dtdx * ((Fx[c] - Fx[cxm]) + (Fy[c] - Fy[cym]) + (Fz[c] - Fz[czm]));
+        }
+        if (out[0] < T(kMIN_DENS)) {
+            out[0] = T(kMIN_DENS);
+            atomicAdd(floor_hits, 1ull);
+        }
+        int cxmym = C(im, jm, k), cxmzm = C(im, j, km), cymzm = C(i, jm, km);
+        T bx = ct_bx(S0, E, n, dtdx, c, cym, czm);
+        T by = ct_by(S0, E, n, dtdx, c, czm, cxm);
+        T bz = ct_bz(S0, E, n, dtdx, c, cxm, cym);
+        T bxm = ct_bx(S0, E, n, dtdx, cxm, cxmym, cxmzm);
+        T bym = ct_by(S0, E, n, dtdx, cym, cymzm, cxmym);
+        T bzm = ct_bz(S0, E, n, dtdx, czm, cxmzm, cymzm);
+        T bxc = T(0.5) * (bx + bxm);
+        T byc = T(0.5) * (by + bym);
+        T bzc = T(0.5) * (bz + bzm);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
+        fld(Sout, 4, n)[c] = bxc;
+        fld(Sout, 5, n)[c] = byc;
+        fld(Sout, 6, n)[c] = bzc;
+        fld(Sout, 7, n)[c] = bx;
+        fld(Sout, 8, n)[c] = by;
+        fld(Sout, 9, n)[c] = bz;
+        if (do_cfl) cmax = (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr);
+        if (!(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
+              isfinite(by) && isfinite(bz)))
+            atomicOr(status, 2u);
+    }
+    if (do_cfl) warp_atomic_max(cmax_bits, cmax);
+}
+
+// ============================================================ passive scalars
+// Upwind flux of compute_fluxes_1d (passive_mod.f90:594-627).
+template <class T>
+__device__ __forceinline__ T upwind_flux(T uL, T uR, T vavg) {
+    T theta = (vavg >= T(0)) ? T(1) : T(-1);
+    return T(0.5) * ((T(1) + theta) * uL + (T(1) - theta) * uR);
+}
+template <class T>
+__device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int comp) {
+    T irho = T(1) / fld(S, 0, n)[c];
+    return fld(S, 1 + comp, n)[c] * irho;
+}
+
+// Predictor: s_h = s - (dt/2dx) sum_d v_d (F_d(i+1/2) - F_d(i-1/2)) with
+// first-order upwind fluxes and the step-start velocity (passive_mod.f90:
+// 133-157, 204-224, 562-590).
+template <class T>
+__global__ void __launch_bounds__(128) k_passive_pred(const T* __restrict__ S0, T* __restrict__ SH, Dims dm,
+                                                      int npass, const Scalars* __restrict__ sc, double dx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i >= dm.nx) return;
+    const int n = dm.n;
+    T dtdx = (T)(0.5 * sc->dt / dx);
+    auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
+    int c = C(i, j, k);
+    int cm[3] = {C(wrap_dn(i, dm.nx), j, k), C(i, wrap_dn(j, dm.ny), k), C(i, j, wrap_dn(k, dm.nz))};
+    int cp[3] = {C(wrap_up(i, dm.nx), j, k), C(i, wrap_up(j, dm.ny), k), C(i, j, wrap_up(k, dm.nz))};
+    T v0[3], vm[3], vp[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        v0[d] = vel_of(S0, n, c, d);
+        vm[d] = vel_of(S0, n, cm[d], d);
+        vp[d] = vel_of(S0, n, cp[d], d);
+    }
+    for (int p = 0; p < npass; ++p) {
+        const T* s = fld(S0, 10 + p, n);
+        T s0 = s[c];
+        T dF[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            T Fp = upwind_flux(s0, s[cp[d]], T(0.5) * (v0[d] + vp[d]));
+            T Fm = upwind_flux(s[cm[d]], s0, T(0.5) * (vm[d] + v0[d]));
+            dF[d] = Fp - Fm;
+        }
+        fld(SH, p, n)[c] = s0 - dtdx * (v0[0] * dF[0] + v0[1] * dF[1] + v0[2] * dF[2]);
+    }
+}
+
+// minmod slope (passive_mod.f90:517-532)
+template <class T>
+__device__ __forceinline__ T minmod(T wm, T w0, T wp) {
+    T dL = w0 - wm;
+    T dR = wp - w0;
+    return T(0.5) * (sgn1(dL) + sgn1(dR)) * vmin(fabs(dL), fabs(dR));
+}
+
+// Corrector: MUSCL states from s_h, upwinded by the time-averaged velocity
+// vel_tavg = (v_old + v_new)/2, applied to the step-start scalar
+// (passive_mod.f90:159-201, 227-239).  mbnd holds, on drive steps, the
+// unforced momentum of the boundary planes: [D][0] plane a = 0 and [D][1]
+// plane a = n-1 of each axis (the ghost images the reference reads).
+template <class T>
+__device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict__ S1, int n, int c, int comp,
+                                   const T* unforced_m) {
+    T vold = vel_of(S0, n, c, comp);
+    T irho = T(1) / fld(S1, 0, n)[c];
+    T m1 = unforced_m ? *unforced_m : fld(S1, 1 + comp, n)[c];
+    return T(0.5) * (vold + m1 * irho);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_passive_corr(const T* __restrict__ S0, const T* __restrict__ SH,
+                                                      T* __restrict__ S1, Dims dm, int npass,
+                                                      const Scalars* __restrict__ sc, double dx, int drive,
+                                                      const T* __restrict__ mbnd, int plane_stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    if (i >= dm.nx) return;
+    const int n = dm.n;
+    T dtdx = (T)(sc->dt / dx);
+    auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
+    int idx[3] = {i, j, k};
+    int nn[3] = {dm.nx, dm.ny, dm.nz};
+    int c = C(i, j, k);
+    int cm[3], cp[3], cm2[3], cp2[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        int t[3] = {i, j, k};
+        t[d] = wrap_dn(idx[d], nn[d]); cm[d] = C(t[0], t[1], t[2]);
+        t[d] = wrap_any(idx[d] - 2, nn[d]); cm2[d] = C(t[0], t[1], t[2]);
+        t[d] = wrap_up(idx[d], nn[d]); cp[d] = C(t[0], t[1], t[2]);
+        t[d] = wrap_any(idx[d] + 2, nn[d]); cp2[d] = C(t[0], t[1], t[2]);
+    }
+    T vt0[3], vtm[3], vtp[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        vt0[d] = vtavg(S0, S1, n, c, d, (const T*)nullptr);
+        const T* um = nullptr;
+        const T* up = nullptr;
+        if (drive) {
+            // transverse position of the cell inside the boundary plane of axis d
+            int a = (d == 0) ? j : i;
+            int b = (d == 2) ? j : k;
+            int pn = (d == 0) ? dm.ny : dm.nx;
+            int pofs = a + pn * b;
+            if (idx[d] == 0) um = mbnd + (size_t)(2 * d + 1) * plane_stride + pofs;            // ghost = plane n-1
+            if (idx[d] == nn[d] - 1) up = mbnd + (size_t)(2 * d + 0) * plane_stride + pofs;    // ghost = plane 0
+        }
+        vtm[d] = vtavg(S0, S1, n, cm[d], d, um);
+        vtp[d] = vtavg(S0, S1, n, cp[d], d, up);
+    }
+    for (int p = 0; p < npass; ++p) {
+        const T* s = fld(SH, p, n);
+        T s0 = s[c];
+        T dF[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            T sm = s[cm[d]], sp = s[cp[d]], sm2 = s[cm2[d]], sp2 = s[cp2[d]];
+            T dlm = minmod(sm2, sm, s0);
+            T dl0 = minmod(sm, s0, sp);
+            T dlp = minmod(s0, sp, sp2);
+            T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vt0[d] + vtp[d]));
+            T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vtm[d] + vt0[d]));
+            dF[d] = Fp - Fm;
+        }
+        fld(S1, 10 + p, n)[c] = fld(S0, 10 + p, n)[c] - dtdx * (vt0[0] * dF[0] + vt0[1] * dF[1] + vt0[2] * dF[2]);
+    }
+}
+
+// ============================================================ forcing
+// get_rho_turb sums (turb_driver_mod.f90:158-186) over the step-start state,
+// per-block partial sums in FP64, reduced in a fixed order by k_force_reduce.
+template <class T>
+__global__ void __launch_bounds__(256) k_force_sums(const T* __restrict__ S0, const T* __restrict__ delv, Dims dm,
+                                                    double* __restrict__ partials) {
+    const int n = dm.n;
+    double s[5] = {0, 0, 0, 0, 0};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double rho = (double)fld(S0, 0, n)[c];
+        double d1 = (double)delv[c], d2 = (double)delv[(size_t)n + c], d3 = (double)delv[2 * (size_t)n + c];
+        s[0] += rho * (d1 * d1 + d2 * d2 + d3 * d3);
+        s[1] += d1 * (double)fld(S0, 1, n)[c] + d2 * (double)fld(S0, 2, n)[c] + d3 * (double)fld(S0, 3, n)[c];
+        s[2] += rho * d1;
+        s[3] += rho * d2;
+        s[4] += rho * d3;
+    }
+    __shared__ double red[5][8];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        double v = warp_sum(s[q]);
+        if (lane == 0) red[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * 5 + threadIdx.x] = v;
+    }
+}
+
+// Sum the per-block partials in block order, then the normalisation of
+// add_random_force (turb_driver_mod.f90:411-434) for one rank.
+static __global__ void k_force_reduce(const double* __restrict__ partials, int nblocks, Scalars* sc, double dx, double edot,
+                               double dt_turb) {
+    __shared__ double acc[5][32];
+    int t = threadIdx.x;   // 32 threads
+    for (int q = 0; q < 5; ++q) {
+        double v = 0.0;
+        for (int b = t; b < nblocks; b += 32) v += partials[(size_t)b * 5 + q];
+        acc[q][t] = v;
+    }
+    __syncwarp();
+    if (t == 0) {
+        double s[5];
+        for (int q = 0; q < 5; ++q) {
+            double v = 0.0;
+            for (int w = 0; w < 32; ++w) v += acc[q][w];
+            s[q] = v;
+        }
+        s[0] = 0.5 * s[0];
+        for (int q = 0; q < 5; ++q) sc->sums[q] = s[q];
+        double dx3 = dx * dx * dx;
+        if (s[0] <= 1.0e-20) {
+            sc->status |= 8u;
+            sc->constE = 0.0;
+            sc->mavg[0] = sc->mavg[1] = sc->mavg[2] = 0.0;
+            return;
+        }
+        sc->mavg[0] = s[2] * dx3;
+        sc->mavg[1] = s[3] * dx3;
+        sc->mavg[2] = s[4] * dx3;
+        double tmp1 = edot * dt_turb / dx3;
+        double tmp2 = sqrt(s[1] * s[1] + (4.0 * tmp1 * s[0]));
+        sc->constE = 0.5 * (-s[1] + tmp2) / s[0];
+    }
+}
+
+// Kick m += constE (rho0 delv - <rho delv>) on the new state
+// (turb_driver_mod.f90:437-453), delv_max, the CFL maximum of the kicked
+// state, and the unforced boundary-plane momentum for k_passive_corr.
+template <class T>
+__global__ void __launch_bounds__(128) k_force_kick(const T* __restrict__ S0, T* __restrict__ S1,
+                                                    const T* __restrict__ delv, Dims dm, Scalars* sc, T asqr,
+                                                    T* __restrict__ mbnd, int plane_stride, int save_bnd) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    bool valid = i < dm.nx;
+    double dvmax = 0.0, cmax = 0.0;
+    if (valid) {
+        const int n = dm.n;
+        int c = i + dm.nx * (j + dm.ny * k);
+        if (save_bnd) {
+            int idx[3] = {i, j, k};
+            int nn[3] = {dm.nx, dm.ny, dm.nz};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                int a = (d == 0) ? j : i;
+                int b = (d == 2) ? j : k;
+                int pn = (d == 0) ? dm.ny : dm.nx;
+                int pofs = a + pn * b;
+                if (idx[d] == 0) mbnd[(size_t)(2 * d + 0) * plane_stride + pofs] = fld(S1, 1 + d, n)[c];
+                if (idx[d] == nn[d] - 1) mbnd[(size_t)(2 * d + 1) * plane_stride + pofs] = fld(S1, 1 + d, n)[c];
+            }
+        }
+        double constE = sc->constE;
+        double r0 = (double)fld(S0, 0, n)[c];
+        double dmx = constE * (r0 * (double)delv[c] - sc->mavg[0]);
+        double dmy = constE * (r0 * (double)delv[(size_t)n + c] - sc->mavg[1]);
+        double dmz = constE * (r0 * (double)delv[2 * (size_t)n + c] - sc->mavg[2]);
+        T mx = (T)((double)fld(S1, 1, n)[c] + dmx);
+        T my = (T)((double)fld(S1, 2, n)[c] + dmy);
+        T mz = (T)((double)fld(S1, 3, n)[c] + dmz);
+        fld(S1, 1, n)[c] = mx;
+        fld(S1, 2, n)[c] = my;
+        fld(S1, 3, n)[c] = mz;
+        dvmax = vmax(vmax(vmax(dvmax, fabs(dmx) / r0), fabs(dmy) / r0), fabs(dmz) / r0);
+        cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
+                                      fld(S1, 6, n)[c], asqr);
+    }
+    warp_atomic_max(&sc->dvmax_bits, dvmax);
+    warp_atomic_max(&sc->cmax_bits, cmax);
+}
+
+// ============================================================ dt and maxima
+// compute_new_time_step (driver.f90:432-448) with the smax coupling of
+// get_max_speed_vanleer (vanleer_mod.f90:3323); resets the step maxima.
+static __global__ void k_finalize(Scalars* sc, double cour, double dx, int drive) {
+    double cell = __longlong_as_double((long long)sc->cmax_bits);
+    double smax = __longlong_as_double((long long)sc->smax_bits);
+    double dvm = __longlong_as_double((long long)sc->dvmax_bits);
+    double cmax = vmax(cell, smax + dvm);
+    if (!(cmax == cmax) || cmax > 1.0e300) sc->status |= 2u;
+    if (cmax < kZERO) sc->status |= 4u;
+    double c = drive ? 0.5 * cour : cour;
+    sc->cmax = cmax;
+    sc->smax_last = smax;
+    sc->dvmax_last = dvm;
+    sc->dt_next = c * dx / cmax;
+    sc->smax_bits = 0ull;
+    sc->cmax_bits = 0ull;
+    sc->dvmax_bits = 0ull;
+}
+
+// cell fast-speed maximum of a state (imhd_max_speed)
+template <class T>
+__global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T asqr, unsigned long long* out_bits) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y, k = blockIdx.z;
+    double cm = 0.0;
+    if (i < dm.nx) {
+        const int n = dm.n;
+        int c = i + dm.nx * (j + dm.ny * k);
+        cm = (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],
+                                    fld(S, 4, n)[c], fld(S, 5, n)[c], fld(S, 6, n)[c], asqr);
+    }
+    warp_atomic_max(out_bits, cm);
+}
+
+// ============================================================ diagnostics
+// compute_KE (driver.f90:518-553) and compute_divB (:492-515) as FP64
+// per-block partials; reduced by k_diag_reduce in block order.
+template <class T>
+__global__ void __launch_bounds__(256) k_diag(const T* __restrict__ S, Dims dm, double* __restrict__ partials) {
+    const int n = dm.n;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        int i = c % dm.nx, j = (c / dm.nx) % dm.ny, k = c / (dm.nx * dm.ny);
+        double rho = vmin(vmax((double)fld(S, 0, n)[c], 1.0e-15), 1.0e10);
+        double mx = (double)fld(S, 1, n)[c], my = (double)fld(S, 2, n)[c], mz = (double)fld(S, 3, n)[c];
+        double vsqr = vmin((mx * mx + my * my + mz * mz) / (rho * rho), 1.0e5);
+        s[1] += vsqr;
+        s[0] += rho * vsqr;
+        s[2] += mx; s[3] += my; s[4] += mz;
+        int cxm = wrap_dn(i, dm.nx) + dm.nx * (j + dm.ny * k);
+        int cym = i + dm.nx * (wrap_dn(j, dm.ny) + dm.ny * k);
+        int czm = i + dm.nx * (j + dm.ny * wrap_dn(k, dm.nz));
+        s[5] += ((double)fld(S, 7, n)[c] - (double)fld(S, 7, n)[cxm]) + ((double)fld(S, 8, n)[c] - (double)fld(S, 8, n)[cym]) +
+                ((double)fld(S, 9, n)[c] - (double)fld(S, 9, n)[czm]);
+    }
+    __shared__ double red[6][8];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        double v = warp_sum(s[q]);
+        if (lane == 0) red[q][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double v = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        partials[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+    }
+}
+
+static __global__ void k_diag_reduce(const double* __restrict__ partials, int nblocks, Scalars* sc, double dx) {
+    if (threadIdx.x != 0) return;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < nblocks; ++b)
+        for (int q = 0; q < 6; ++q) s[q] += partials[(size_t)b * 6 + q];
+    double dx3 = dx * dx * dx;
+    sc->diag[0] = 0.5 * s[0] * dx3;
+    sc->diag[1] = s[1] * dx3;
+    sc->diag[2] = s[2] * dx3;
+    sc->diag[3] = s[3] * dx3;
+    sc->diag[4] = s[4] * dx3;
+    sc->diag[5] = s[5];
+}
+
+// ============================================================ host transfer
+template <class T>
+__global__ void k_from_f64(const double* __restrict__ src, T* __restrict__ dst, int n) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = (T)src[c];
+}
+template <class T>
+__global__ void k_to_f64(const T* __restrict__ src, double* __restrict__ dst, int n) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) dst[c] = (double)src[c];
+}
+
+}  // namespace imhd

@@ -1,0 +1,136 @@
+"""Parity of the CUDA step (through the C ABI) with the FP64 oracle.
+
+FP64: bit-exact (every state array, every dt and the interface wave-speed
+maximum) on undriven runs; the drive step's FP64 sums are reduced in a
+different order on the GPU, so driven runs are held to relative L1 <= 1e-12
+per field.  FP32: relative L1 <= 1e-5 per field against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from helpers import gpu_run, oracle_run, rel_l1
+from isothermal_mhd_b200 import problems
+
+pytestmark = pytest.mark.gpu
+
+SOLVERS = ["roe", "hlld", "hlle"]
+
+
+def assert_exact(g, o):
+    for name in ("q", "b"):
+        assert np.array_equal(g[name], o[name]), (name, np.max(np.abs(g[name] - o[name])))
+    if o["p"] is not None:
+        assert np.array_equal(g["p"], o["p"]), ("p", np.max(np.abs(g["p"] - o["p"])))
+    assert g["dts"] == o["dts"]
+    assert g["smax"] == o["smax"]
+    assert g["dt_next"] == o["dt_next"]
+
+
+@pytest.mark.parametrize("riemann", SOLVERS)
+def test_fp64_bit_exact_smooth_16(riemann):
+    n = 16
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, riemann, steps=6)
+    g = gpu_run(ic, n, riemann, steps=6)
+    assert_exact(g, o)
+
+
+@pytest.mark.parametrize("riemann", SOLVERS)
+def test_fp64_bit_exact_noncubic(riemann):
+    n = (16, 24, 20)
+    ic = problems.smooth_wave_box(n, npass=2)
+    o = oracle_run(ic, n, riemann, steps=4)
+    g = gpu_run(ic, n, riemann, steps=4)
+    assert_exact(g, o)
+
+
+@pytest.mark.parametrize("axis", [0, 1, 2])
+def test_fp64_bit_exact_shock(axis):
+    n = 16
+    ic = problems.shock_tube(n, axis=axis, npass=1)
+    o = oracle_run(ic, n, "roe", steps=8)
+    g = gpu_run(ic, n, "roe", steps=8)
+    assert_exact(g, o)
+
+
+@pytest.mark.parametrize("riemann", ["roe", "hlld"])
+def test_fp64_bit_exact_alfven_zero_components(riemann):
+    # exact zeros in velocity and transverse field exercise signed-zero paths
+    n = 16
+    ic = problems.alfven_wave(n, npass=0)
+    o = oracle_run(ic, n, riemann, steps=5, npass=0)
+    g = gpu_run(ic, n, riemann, steps=5, npass=0)
+    assert_exact(g, o)
+
+
+def test_fp64_bit_exact_32_roe():
+    n = 32
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, "roe", steps=20, nthreads=8)
+    g = gpu_run(ic, n, "roe", steps=20)
+    assert_exact(g, o)
+
+
+def test_fp64_padded_layout_matches_unpadded():
+    n = 16
+    ic = problems.smooth_wave_box(n, npass=1)
+    g0 = gpu_run(ic, n, "hlld", steps=3, ng=0)
+    g6 = gpu_run(ic, n, "hlld", steps=3, ng=6)
+    assert np.array_equal(g0["q"], g6["q"]) and np.array_equal(g0["b"], g6["b"])
+    assert np.array_equal(g0["p"], g6["p"])
+
+
+def test_download_fills_ghosts_periodically():
+    from isothermal_mhd_b200 import Box
+    n, g = 12, 6
+    q, b, p = problems.smooth_wave_box(n, npass=1)
+    with Box(n, precision=64, riemann="roe", npass=1, ng=g, ng_pass=4) as box:
+        box.upload(problems.pad(q, g), problems.pad(b, g), problems.pad(p, 4))
+        qd, bd, pd = box.download()
+    assert np.array_equal(qd, problems.pad(q, g))
+    assert np.array_equal(bd, problems.pad(b, g))
+    assert np.array_equal(pd, problems.pad(p, 4))
+
+
+@pytest.mark.parametrize("riemann", ["roe", "hlld"])
+def test_fp64_driven_ref_forcing(riemann):
+    from oracle.pyoracle import Oracle
+    n = 16
+    ic = problems.smooth_wave_box(n, npass=1)
+    gen = Oracle(n, riemann=riemann, npass=1)
+    delv = gen.generate_ref_force(seeds=(1234, 5678, 9123))
+    gen.close()
+    o = oracle_run(ic, n, riemann, steps=5, force=delv, drive_at=(1, 3), edot=1.0)
+    g = gpu_run(ic, n, riemann, steps=5, force=delv, drive_at=(1, 3), edot=1.0, dts=o["dts"])
+    for name in ("q", "b", "p"):
+        err = rel_l1(g[name], o[name])
+        assert np.all(err <= 1e-12), (name, err)
+    assert abs(g["dt_next"] - o["dt_next"]) <= 1e-12 * o["dt_next"]
+
+
+@pytest.mark.parametrize("riemann", SOLVERS)
+def test_fp32_within_1e5_of_fp64_oracle(riemann):
+    n = 32
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, riemann, steps=20, nthreads=8)
+    g = gpu_run(ic, n, riemann, steps=20, precision=32, dts=o["dts"])
+    for name in ("q", "b", "p"):
+        ref = o[name]
+        err = rel_l1(g[name], ref)
+        # fields that are identically zero in the reference are judged in absolute terms
+        assert np.all(err <= 1e-5), (name, err)
+
+
+def test_uniform_state_stays_uniform_fp32_128():
+    from isothermal_mhd_b200 import Box
+    n = 128
+    q, b, p = problems.uniform_box(n, rho=1.3, v=(0.2, -0.1, 0.05), b0=(0.4, 0.3, -0.2), npass=2, pass_value=0.25)
+    with Box(n, precision=32, riemann="roe", npass=2) as box:
+        box.upload(q, b, p)
+        dt = 1e-15
+        for _ in range(3):
+            dt = box.step(dt)
+        qg, bg, pg = box.download()
+    np.testing.assert_array_equal(qg, q.astype(np.float32).astype(np.float64))
+    np.testing.assert_array_equal(bg, b.astype(np.float32).astype(np.float64))
+    np.testing.assert_array_equal(pg, p.astype(np.float32).astype(np.float64))
