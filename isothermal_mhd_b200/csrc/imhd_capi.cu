@@ -339,12 +339,17 @@ int imhd_max_speed(imhd_box* x, double* cmax) {
     if (!x || !cmax) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
     CK(is64(x) ? imhd::run_max_speed<double>(x->b) : imhd::run_max_speed<float>(x->b));
-    unsigned long long bits = 0;
-    CK(cudaMemcpyAsync(x->hio + 3, &x->b.sc->cfl0_bits, 8, cudaMemcpyDeviceToHost, x->b.st));
+    unsigned long long slots[imhd::kSlots];
+    CK(cudaMemcpyAsync(slots, x->b.sc->cfl_slots, sizeof(slots), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
-    std::memcpy(&bits, x->hio + 3, 8);
-    std::memcpy(cmax, &bits, 8);
+    double m = 0.0;
+    for (int s = 0; s < imhd::kSlots; ++s) {
+        double v;
+        std::memcpy(&v, &slots[s], 8);
+        if (v != v || v > m) m = v;
+    }
+    *cmax = m;
     return IMHD_OK;
 }
 

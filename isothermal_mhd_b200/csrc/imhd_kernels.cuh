@@ -39,9 +39,13 @@ __device__ __forceinline__ const T* fld(const T* S, int f, int n) { return S + (
 template <class T>
 __device__ __forceinline__ T* fld(T* S, int f, int n) { return S + (size_t)f * (size_t)n; }
 
+// max that keeps a NaN (speeds are otherwise >= 0, so the order of a max
+// reduction does not change its value)
+__device__ __forceinline__ double nmax(double a, double b) { return (a != a || a > b) ? a : b; }
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = vmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
 __device__ __forceinline__ double warp_sum(double v) {
@@ -49,11 +53,23 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-// all 32 lanes of the warp must call this
-__device__ __forceinline__ void warp_atomic_max(unsigned long long* addr, double v) {
+// Block-wide max folded into slots[block id mod kSlots] with one atomicMax on
+// the bit pattern (NaN bits exceed every finite non-negative double).  Every
+// thread of the block must call it (it synchronises the block).
+template <int NT>
+__device__ __forceinline__ void block_atomic_max(unsigned long long* slots, double v) {
+    __shared__ double red[NT / 32];
     v = warp_max(v);
-    if ((threadIdx.x & 31) == 0 && !(v <= 0.0))   // NaN bits exceed every finite value
-        atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+#pragma unroll
+        for (int w = 1; w < NT / 32; ++w) m = nmax(m, red[w]);
+        unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        if (!(m <= 0.0)) atomicMax(&slots[bid % kSlots], (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
 }
 
 // rotated field indices of sweep D (vanleer_mod.f90:443-461, 605-630, 784-806)
@@ -68,7 +84,7 @@ template <int D> struct Rot {
 // the cell values, the normal field the face value.
 template <class T, int SOLVER, int D>
 __global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
-                                                   T asqr, unsigned long long* smax_bits) {
+                                                   T asqr, unsigned long long* smax_slots) {
     using R = Rot<D>;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y, k = blockIdx.z;
@@ -97,7 +113,7 @@ __global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* _
         Fd[4 * (size_t)dm.n + c] = Fo[5];
         Fd[5 * (size_t)dm.n + c] = Fo[6];
     }
-    warp_atomic_max(smax_bits, (double)smax);
+    block_atomic_max<128>(smax_slots, (double)smax);
 }
 
 // ============================================================ corrector flux
@@ -134,7 +150,7 @@ __device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int 
 // registers.  Loads stay coalesced along x.
 template <class T, int SOLVER, int D>
 __global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S, T* __restrict__ F, Dims dm,
-                                                         int seg, T cs, T asqr, unsigned long long* smax_bits) {
+                                                         int seg, T cs, T asqr, unsigned long long* smax_slots) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int o = blockIdx.y;                         // k for D=1, j for D=2
     int a0 = blockIdx.z * seg;
@@ -168,14 +184,14 @@ __global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S
             bnA = bnB; bnB = bnC;
         }
     }
-    warp_atomic_max(smax_bits, (double)smax);
+    block_atomic_max<128>(smax_slots, (double)smax);
 }
 
 // Sweep along x: a block covers TX faces of one (j,k) row; primitives of the
 // TX+3 cells and the TX+1 slopes are staged in shared memory.
 template <class T, int SOLVER, int TX>
 __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
-                                                    T asqr, unsigned long long* smax_bits) {
+                                                    T asqr, unsigned long long* smax_slots) {
     __shared__ T sw[6][TX + 3];
     __shared__ T sbn[TX + 3];
     __shared__ T sd[6][TX + 1];
@@ -214,7 +230,7 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* 
         riemann<SOLVER>(qL, qR, cs, asqr, Fo, smax);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
-    warp_atomic_max(smax_bits, (double)smax);
+    block_atomic_max<128>(smax_slots, (double)smax);
 }
 
 // ============================================================ corner EMF
@@ -229,6 +245,16 @@ __device__ __forceinline__ T ecc(const T* __restrict__ S, int n, int c, int comp
     if (comp == 0) return (by * mz - bz * my) * irho;
     if (comp == 1) return (bz * mx - bx * mz) * irho;
     return (bx * my - by * mx) * irho;
+}
+// all three components of the cell-centre EMF of one cell (one reciprocal)
+template <class T>
+__device__ __forceinline__ void ecc3(const T* __restrict__ S, int n, int c, T& ex, T& ey, T& ez) {
+    T irho = T(1) / fld(S, 0, n)[c];
+    T mx = fld(S, 1, n)[c], my = fld(S, 2, n)[c], mz = fld(S, 3, n)[c];
+    T bx = fld(S, 4, n)[c], by = fld(S, 5, n)[c], bz = fld(S, 6, n)[c];
+    ex = (by * mz - bz * my) * irho;
+    ey = (bz * mx - bx * mz) * irho;
+    ez = (bx * my - by * mx) * irho;
 }
 template <class T>
 __device__ __forceinline__ T face_v(const T* __restrict__ S, int n, int c, int cn, int comp) {
@@ -262,11 +288,16 @@ __global__ void __launch_bounds__(128) k_corner_emf(const T* __restrict__ S, con
     T vx = face_v(S, n, c000, c100, 0);
     T vy = face_v(S, n, c000, c010, 1);
     T vz = face_v(S, n, c000, c001, 2);
+    T e000x, e000y, e000z, e100x, e100y, e100z, e010x, e010y, e010z, e001x, e001y, e001z;
+    ecc3(S, n, c000, e000x, e000y, e000z);
+    ecc3(S, n, c100, e100x, e100y, e100z);
+    ecc3(S, n, c010, e010x, e010y, e010z);
+    ecc3(S, n, c001, e001x, e001y, e001z);
     // Ez at (i+1/2, j+1/2, k)
     {
         T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
         T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
-        T E33_000 = ecc(S, n, c000, 2), E33_100 = ecc(S, n, c100, 2), E33_010 = ecc(S, n, c010, 2), E33_110 = ecc(S, n, c110, 2);
+        T E33_000 = e000z, E33_100 = e100z, E33_010 = e010z, E33_110 = ecc(S, n, c110, 2);
         T dyL14 = T(2) * (E32_000 - E33_000);
         T dyR14 = T(2) * (E32_100 - E33_100);
         T dyL34 = T(2) * (E33_010 - E32_000);
@@ -286,7 +317,7 @@ __global__ void __launch_bounds__(128) k_corner_emf(const T* __restrict__ S, con
     {
         T E21_000 = Fx_bt2[c000], E21_001 = Fx_bt2[c001];
         T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
-        T E23_000 = ecc(S, n, c000, 1), E23_100 = ecc(S, n, c100, 1), E23_001 = ecc(S, n, c001, 1), E23_101 = ecc(S, n, c101, 1);
+        T E23_000 = e000y, E23_100 = e100y, E23_001 = e001y, E23_101 = ecc(S, n, c101, 1);
         T dzL14 = T(2) * (E22_000 - E23_000);
         T dzR14 = T(2) * (E22_100 - E23_100);
         T dzL34 = T(2) * (E23_001 - E22_000);
@@ -306,7 +337,7 @@ __global__ void __launch_bounds__(128) k_corner_emf(const T* __restrict__ S, con
     {
         T E11_000 = -Fy_bt1[c000], E11_001 = -Fy_bt1[c001];
         T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
-        T E13_000 = ecc(S, n, c000, 0), E13_010 = ecc(S, n, c010, 0), E13_001 = ecc(S, n, c001, 0), E13_011 = ecc(S, n, c011, 0);
+        T E13_000 = e000x, E13_010 = e010x, E13_001 = e001x, E13_011 = ecc(S, n, c011, 0);
         T dzL14 = T(2) * (E12_000 - E13_000);
         T dzR14 = T(2) * (E12_010 - E13_010);
         T dzL34 = T(2) * (E13_001 - E12_000);
@@ -349,7 +380,7 @@ template <class T>
 __global__ void __launch_bounds__(128) k_update(const T* __restrict__ S0, const T* __restrict__ F,
                                                 const T* __restrict__ E, T* __restrict__ Sout, Dims dm,
                                                 const Scalars* __restrict__ sc, double dt_scale, double dx, T asqr,
-                                                int do_cfl, unsigned long long* cmax_bits,
+                                                int do_cfl, unsigned long long* cmax_slots,
                                                 unsigned long long* floor_hits, unsigned int* status) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y, k = blockIdx.z;
@@ -400,7 +431,7 @@ __global__ void __launch_bounds__(128) k_update(const T* __restrict__ S0, const 
               isfinite(by) && isfinite(bz)))
             atomicOr(status, 2u);
     }
-    if (do_cfl) warp_atomic_max(cmax_bits, cmax);
+    if (do_cfl) block_atomic_max<128>(cmax_slots, cmax);
 }
 
 // ============================================================ passive scalars
@@ -644,17 +675,23 @@ __global__ void __launch_bounds__(128) k_force_kick(const T* __restrict__ S0, T*
         cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
                                       fld(S1, 6, n)[c], asqr);
     }
-    warp_atomic_max(&sc->dvmax_bits, dvmax);
-    warp_atomic_max(&sc->cmax_bits, cmax);
+    block_atomic_max<128>(sc->dvmax_slots, dvmax);
+    block_atomic_max<128>(sc->cmax_slots, cmax);
 }
 
 // ============================================================ dt and maxima
 // compute_new_time_step (driver.f90:432-448) with the smax coupling of
 // get_max_speed_vanleer (vanleer_mod.f90:3323); resets the step maxima.
 static __global__ void k_finalize(Scalars* sc, double cour, double dx, int drive) {
-    double cell = __longlong_as_double((long long)sc->cmax_bits);
-    double smax = __longlong_as_double((long long)sc->smax_bits);
-    double dvm = __longlong_as_double((long long)sc->dvmax_bits);
+    double cell = 0.0, smax = 0.0, dvm = 0.0;
+    for (int s = 0; s < kSlots; ++s) {
+        cell = nmax(cell, __longlong_as_double((long long)sc->cmax_slots[s]));
+        smax = nmax(smax, __longlong_as_double((long long)sc->smax_slots[s]));
+        dvm = nmax(dvm, __longlong_as_double((long long)sc->dvmax_slots[s]));
+        sc->cmax_slots[s] = 0ull;
+        sc->smax_slots[s] = 0ull;
+        sc->dvmax_slots[s] = 0ull;
+    }
     double cmax = vmax(cell, smax + dvm);
     if (!(cmax == cmax) || cmax > 1.0e300) sc->status |= 2u;
     if (cmax < kZERO) sc->status |= 4u;
@@ -663,14 +700,11 @@ static __global__ void k_finalize(Scalars* sc, double cour, double dx, int drive
     sc->smax_last = smax;
     sc->dvmax_last = dvm;
     sc->dt_next = c * dx / cmax;
-    sc->smax_bits = 0ull;
-    sc->cmax_bits = 0ull;
-    sc->dvmax_bits = 0ull;
 }
 
 // cell fast-speed maximum of a state (imhd_max_speed)
 template <class T>
-__global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T asqr, unsigned long long* out_bits) {
+__global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T asqr, unsigned long long* out_slots) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y, k = blockIdx.z;
     double cm = 0.0;
@@ -680,7 +714,7 @@ __global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T
         cm = (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],
                                     fld(S, 4, n)[c], fld(S, 5, n)[c], fld(S, 6, n)[c], asqr);
     }
-    warp_atomic_max(out_bits, cm);
+    block_atomic_max<128>(out_slots, cm);
 }
 
 // ============================================================ diagnostics

@@ -28,9 +28,9 @@ static void launch_fluxes_pred(BoxDev& b) {
     T* F = (T*)b.F;
     T cs = (T)b.cs, asqr = (T)(b.cs * b.cs);
     mark(b, kStPredFlux);
-    k_pred_flux<T, SOLVER, 0><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, &b.sc->smax_bits);
-    k_pred_flux<T, SOLVER, 1><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, &b.sc->smax_bits);
-    k_pred_flux<T, SOLVER, 2><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, &b.sc->smax_bits);
+    k_pred_flux<T, SOLVER, 0><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+    k_pred_flux<T, SOLVER, 1><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+    k_pred_flux<T, SOLVER, 2><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
     b.launches += 3;
 }
 
@@ -42,13 +42,13 @@ static void launch_fluxes_corr(BoxDev& b) {
     T cs = (T)b.cs, asqr = (T)(b.cs * b.cs);
     dim3 gx((dm.nx + kTX - 1) / kTX, dm.ny, dm.nz);
     mark(b, kStCorrFluxX);
-    k_corr_flux_x<T, SOLVER, kTX><<<gx, kTX, 0, b.st>>>(S, F, dm, cs, asqr, &b.sc->smax_bits);
+    k_corr_flux_x<T, SOLVER, kTX><<<gx, kTX, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
     dim3 gy((dm.nx + kBX - 1) / kBX, dm.nz, (dm.ny + kSeg - 1) / kSeg);
     mark(b, kStCorrFluxY);
-    k_corr_flux_march<T, SOLVER, 1><<<gy, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, &b.sc->smax_bits);
+    k_corr_flux_march<T, SOLVER, 1><<<gy, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, b.sc->smax_slots);
     dim3 gz((dm.nx + kBX - 1) / kBX, dm.ny, (dm.nz + kSeg - 1) / kSeg);
     mark(b, kStCorrFluxZ);
-    k_corr_flux_march<T, SOLVER, 2><<<gz, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, &b.sc->smax_bits);
+    k_corr_flux_march<T, SOLVER, 2><<<gz, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, b.sc->smax_slots);
     b.launches += 3;
 }
 
@@ -76,7 +76,7 @@ cudaError_t run_step(BoxDev& b, int drive) {
     k_corner_emf<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (T*)b.E, dm);
     mark(b, kStPredUpdate);
     k_update<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (const T*)b.E, Bs, dm, b.sc, 0.5, b.dx, asqr, 0,
-                                       &b.sc->cmax_bits, &b.sc->floor_hits, &b.sc->status);
+                                       b.sc->cmax_slots, &b.sc->floor_hits, &b.sc->status);
     b.launches += 2;
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state into B
@@ -89,7 +89,7 @@ cudaError_t run_step(BoxDev& b, int drive) {
     k_corner_emf<T><<<grd, blk, 0, b.st>>>(Bs, (const T*)b.F, (T*)b.E, dm);
     mark(b, kStFinalUpdate);
     k_update<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (const T*)b.E, Bs, dm, b.sc, 1.0, b.dx, asqr, drive ? 0 : 1,
-                                       &b.sc->cmax_bits, &b.sc->floor_hits, &b.sc->status);
+                                       b.sc->cmax_slots, &b.sc->floor_hits, &b.sc->status);
     b.launches += 2;
     if (drive) {
         mark(b, kStForceKick);
@@ -116,8 +116,8 @@ template <class T>
 cudaError_t run_max_speed(BoxDev& b) {
     const Dims& dm = b.dm;
     dim3 blk(kBX), grd((dm.nx + kBX - 1) / kBX, dm.ny, dm.nz);
-    cudaMemsetAsync(&b.sc->cfl0_bits, 0, sizeof(unsigned long long), b.st);
-    k_cfl<T><<<grd, blk, 0, b.st>>>((const T*)b.A, dm, (T)(b.cs * b.cs), &b.sc->cfl0_bits);
+    cudaMemsetAsync(b.sc->cfl_slots, 0, sizeof(b.sc->cfl_slots), b.st);
+    k_cfl<T><<<grd, blk, 0, b.st>>>((const T*)b.A, dm, (T)(b.cs * b.cs), b.sc->cfl_slots);
     b.launches += 1;
     return cudaGetLastError();
 }

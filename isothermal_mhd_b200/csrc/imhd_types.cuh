@@ -23,13 +23,11 @@ struct Dims {
 
 // Device scalars of one box (FP64; maxima kept as the bit pattern of a
 // non-negative double so that atomicMax on the integer is a max on the value).
+constexpr int kSlots = 64;   // spread of the max reductions over addresses
+
 struct Scalars {
     double dt;                       // current dt (input of every step kernel)
     double dt_next;                  // COUR*dx/cmax of the last step
-    unsigned long long smax_bits;    // interface wave-speed max of the step
-    unsigned long long cmax_bits;    // cell fast-speed max of the final state
-    unsigned long long dvmax_bits;   // delv_max of the forcing kick
-    unsigned long long cfl0_bits;    // cell max of imhd_max_speed
     double sums[5];                  // quad_term1, quad_term2, momx/y/z_avg
     double constE;
     double mavg[3];
@@ -39,6 +37,11 @@ struct Scalars {
     unsigned int status;
     unsigned int pad;
     unsigned long long floor_hits;
+    // per-block maxima land in slot (block id mod kSlots); k_finalize folds them
+    unsigned long long smax_slots[kSlots];
+    unsigned long long cmax_slots[kSlots];
+    unsigned long long dvmax_slots[kSlots];
+    unsigned long long cfl_slots[kSlots];
 };
 
 struct BoxDev {
