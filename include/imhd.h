@@ -151,6 +151,27 @@ int imhd_profile(imhd_box* box, int enable);
 #define IMHD_NSTAGES 13
 int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int reset);
 
+/* One undriven time step, like imhd_step, for callers that cannot allocate
+ * device memory: hosts that own every device buffer (pool allocators,
+ * OpenACC / CUDA Fortran managed arrays), code running inside a CUDA graph
+ * capture, allocation-free real-time loops.  No reference counterpart: the
+ * reference allocates its work arrays itself (vanleer_mod.f90:169-244).
+ * The caller passes device buffers: state_in (read) and state_out (written),
+ * distinct, each 10 + npass fields of nx*ny*nz elements of the precision's
+ * type in the library's layout (rho, mx, my, mz, Bx_cc, By_cc, Bz_cc,
+ * Bx_face, By_face, Bz_face, passive scalars; x fastest).  dt is read from
+ * the host, *dt_next (host) receives COUR*dx/cmax, stream may be NULL.
+ * The step's work arrays live in one 48 MiB file-scope device array held by
+ * every GPU that loads the library until exit; boxes needing more
+ * ((21 + npass) * nx*ny*nz * element size + 4 KiB: 64^3 in FP64, about 80^3
+ * in FP32 with two passives) are rejected with IMHD_E_ARG.  All calls on a
+ * device share that array: calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture starts. */
+int imhd_step_static(int precision, int nx, int ny, int nz, int riemann, int npass, double sound_speed,
+                     double cour, const void* state_in, void* state_out, double dt, double* dt_next,
+                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ EXPORTS = (
     "imhd_default_config", "imhd_create", "imhd_upload", "imhd_download", "imhd_set_force",
     "imhd_step", "imhd_max_speed", "imhd_diagnostics", "imhd_status", "imhd_wave_speeds",
     "imhd_destroy", "imhd_last_error", "imhd_launch_count", "imhd_set_stream", "imhd_profile",
-    "imhd_stage_times",
+    "imhd_stage_times", "imhd_step_static",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -89,6 +89,8 @@ def lib():
         L.imhd_profile.restype = i
         L.imhd_stage_times.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), i, i]
         L.imhd_stage_times.restype = i
+        L.imhd_step_static.argtypes = [i, i, i, i, i, i, d, d, vp, vp, d, dp, vp]
+        L.imhd_step_static.restype = i
         _lib = L
     return _lib
 

@@ -30,6 +30,7 @@ UNITS = {
     # denormals flushed; the FP64 pieces of this unit are unaffected
     "imhd_f32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "imhd_capi.cu": [],
+    "imhd_static.cu": [],
 }
 HEADERS = ["imhd_physics.cuh", "imhd_types.cuh", "imhd_kernels.cuh", "imhd_launch.cuh"]
 

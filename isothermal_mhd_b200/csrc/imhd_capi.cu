@@ -157,6 +157,15 @@ int accumulate_stage_times(imhd_box* x) {
 
 }  // namespace
 
+namespace imhd {
+// lets other translation units of the library report through imhd_last_error
+const char* set_last_error(int code, const char* msg) {
+    (void)code;
+    g_err = msg;
+    return g_err.c_str();
+}
+}  // namespace imhd
+
 extern "C" {
 
 void imhd_default_config(imhd_config* c) {
