@@ -32,7 +32,7 @@ UNITS = {
     "imhd_capi.cu": [],
     "imhd_static.cu": [],
 }
-HEADERS = ["imhd_physics.cuh", "imhd_types.cuh", "imhd_kernels.cuh", "imhd_launch.cuh"]
+HEADERS = ["imhd_physics.cuh", "imhd_physics_fast.cuh", "imhd_types.cuh", "imhd_kernels.cuh", "imhd_launch.cuh"]
 
 
 def nvcc() -> str:

@@ -25,7 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "imhd_physics.cuh"
+#include "imhd_physics_fast.cuh"
 #include "imhd_types.cuh"
 
 namespace imhd {
@@ -72,6 +72,22 @@ __device__ __forceinline__ void block_atomic_max(unsigned long long* slots, doub
     __syncthreads();
 }
 
+// Same as block_atomic_max for any blockDim.x that is a multiple of 32.
+__device__ __forceinline__ void block_atomic_max_any(unsigned long long* slots, double v) {
+    __shared__ double red[32];
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        int nw = (int)(blockDim.x >> 5);
+        for (int w = 1; w < nw; ++w) m = nmax(m, red[w]);
+        unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+        if (!(m <= 0.0)) atomicMax(&slots[bid % kSlots], (unsigned long long)__double_as_longlong(m));
+    }
+    __syncthreads();
+}
+
 // rotated field indices of sweep D (vanleer_mod.f90:443-461, 605-630, 784-806)
 template <int D> struct Rot {
     static constexpr int MN = 1 + D, MT1 = 1 + (D + 1) % 3, MT2 = 1 + (D + 2) % 3;
@@ -104,7 +120,7 @@ __global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* _
         uR[3] = fld(S, R::MT2, dm.n)[cn]; uR[4] = uL[4];
         uR[5] = fld(S, R::BT1, dm.n)[cn]; uR[6] = fld(S, R::BT2, dm.n)[cn];
         T Fo[7];
-        riemann<SOLVER>(uL, uR, cs, asqr, Fo, smax);
+        riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, smax);
         T* Fd = F + (size_t)(6 * D) * dm.n;
         Fd[c] = Fo[0];
         Fd[(size_t)dm.n + c] = Fo[1];
@@ -167,17 +183,17 @@ __global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S
         load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wa, tmpbn);
         load_prim<T, D>(S, dm.n, base + a0 * stride, wb_, bnA);
         load_prim<T, D>(S, dm.n, base + wrap_up(a0, na) * stride, wc, bnB);
-        plm_char_slope(wa, wb_, wc, bnA, cs, asqr, dA);
+        char_slope(wa, wb_, wc, bnA, cs, asqr, dA);
         for (int a = a0; a < a1; ++a) {
             int ap1 = wrap_up(a, na);
             int ap2 = wrap_up(ap1, na);
             T bnC;
             load_prim<T, D>(S, dm.n, base + ap2 * stride, wd, bnC);
-            plm_char_slope(wb_, wc, wd, bnB, cs, asqr, dB);
+            char_slope(wb_, wc, wd, bnB, cs, asqr, dB);
             T qL[7], qR[7], Fo[7];
             plm_left_state(wb_, dA, bnA, qL);
             plm_right_state(wc, dB, bnA, qR);
-            riemann<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+            riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
             store_flux(F, D, dm.n, base + a * stride, Fo);
 #pragma unroll
             for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
@@ -211,7 +227,7 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* 
         T wm[6], w0[6], wp[6], d[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) { wm[m] = sw[m][t]; w0[m] = sw[m][t + 1]; wp[m] = sw[m][t + 2]; }
-        plm_char_slope(wm, w0, wp, sbn[t + 1], cs, asqr, d);
+        char_slope(wm, w0, wp, sbn[t + 1], cs, asqr, d);
 #pragma unroll
         for (int m = 0; m < 6; ++m) sd[m][t] = d[m];
     }
@@ -227,10 +243,62 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* 
         T qL[7], qR[7], Fo[7];
         plm_left_state(wl, dl, bn, qL);
         plm_right_state(wr, dr, bn, qR);
-        riemann<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
     block_atomic_max<128>(smax_slots, (double)smax);
+}
+
+// Sweep along x over whole rows: one block per (j,k) row.  The primitives,
+// face fields and slopes of the row live in shared memory and the periodic
+// wrap is an index wrap inside the row, so every cell's slope is computed
+// exactly once (the tiled kernel above recomputes one slope per tile and
+// stages a halo).  Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
+template <class T, int SOLVER>
+__global__ void __launch_bounds__(256) k_corr_flux_xrow(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
+                                                        T asqr, unsigned long long* smax_slots) {
+    extern __shared__ __align__(16) unsigned char xrow_smem[];
+    const int nx = dm.nx;
+    T* sw = (T*)xrow_smem;     // [6][nx] primitives
+    T* sbn = sw + 6 * nx;      // [nx] face field at i+1/2
+    T* sd = sbn + nx;          // [6][nx] slopes
+    int j = blockIdx.x, k = blockIdx.y;
+    int row = nx * (j + dm.ny * k);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        T w[6], bn;
+        load_prim<T, 0>(S, dm.n, row + i, w, bn);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) sw[m * nx + i] = w[m];
+        sbn[i] = bn;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        int im = wrap_dn(i, nx), ip = wrap_up(i, nx);
+        T wm[6], w0[6], wp[6], d[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) { wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip]; }
+        char_slope(wm, w0, wp, sbn[i], cs, asqr, d);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) sd[m * nx + i] = d[m];
+    }
+    __syncthreads();
+    T smax = T(0);
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        int ip = wrap_up(i, nx);
+        T wl[6], wr[6], dl[6], dr[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            wl[m] = sw[m * nx + i]; wr[m] = sw[m * nx + ip];
+            dl[m] = sd[m * nx + i]; dr[m] = sd[m * nx + ip];
+        }
+        T bn = sbn[i];
+        T qL[7], qR[7], Fo[7];
+        plm_left_state(wl, dl, bn, qL);
+        plm_right_state(wr, dr, bn, qR);
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+        store_flux(F, 0, dm.n, row + i, Fo);
+    }
+    block_atomic_max_any(smax_slots, (double)smax);
 }
 
 // ============================================================ corner EMF

@@ -19,6 +19,7 @@ inline void mark(BoxDev& b, int stage) {
 constexpr int kBX = 128;       // threads along x of the per-cell kernels
 constexpr int kTX = 128;       // faces per block of the x sweep
 constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
+constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
 
 template <class T, int SOLVER>
 static void launch_fluxes_pred(BoxDev& b) {
@@ -40,9 +41,23 @@ static void launch_fluxes_corr(BoxDev& b) {
     const T* S = (const T*)b.B;
     T* F = (T*)b.F;
     T cs = (T)b.cs, asqr = (T)(b.cs * b.cs);
-    dim3 gx((dm.nx + kTX - 1) / kTX, dm.ny, dm.nz);
     mark(b, kStCorrFluxX);
-    k_corr_flux_x<T, SOLVER, kTX><<<gx, kTX, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+    size_t row_smem = 13 * (size_t)dm.nx * sizeof(T);
+    if (row_smem <= kRowSmemMax) {
+        static bool attr_set[64] = {};   // per instantiation and device
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+            cudaFuncSetAttribute(k_corr_flux_xrow<T, SOLVER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kRowSmemMax);
+            if (dev >= 0 && dev < 64) attr_set[dev] = true;
+        }
+        int bd = dm.nx >= 256 ? 256 : ((dm.nx + 31) / 32) * 32;
+        k_corr_flux_xrow<T, SOLVER><<<dim3(dm.ny, dm.nz), bd, row_smem, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+    } else {
+        dim3 gx((dm.nx + kTX - 1) / kTX, dm.ny, dm.nz);
+        k_corr_flux_x<T, SOLVER, kTX><<<gx, kTX, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+    }
     dim3 gy((dm.nx + kBX - 1) / kBX, dm.nz, (dm.ny + kSeg - 1) / kSeg);
     mark(b, kStCorrFluxY);
     k_corr_flux_march<T, SOLVER, 1><<<gy, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, b.sc->smax_slots);
