@@ -151,6 +151,45 @@ int imhd_profile(imhd_box* box, int enable);
 #define IMHD_NSTAGES 13
 int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int reset);
 
+/* Fill a box from a sum of Fourier modes on the cell centres,
+ * v_d(x) = sum_m 2 Re(A_{m,d} exp(2 pi i k_m . x)), x = ((i+1/2)/nx, ...):
+ * kvec[3m..3m+2] are integer wave numbers, amp[6m + 2d] / amp[6m + 2d + 1]
+ * the real / imaginary part of A_{m,d}.  target 0 adds rho * scale * v to the
+ * momentum (an initial velocity field), target 1 sets the force field to
+ * scale * v.  The device counterpart of generate_rand_force's inverse DFT
+ * (turb_driver_mod.f90:310-384) for generators whose amplitudes live on the
+ * host, e.g. the Ornstein-Uhlenbeck forcing of isothermal_mhd_b200.forcing. */
+int imhd_fourier_field(imhd_box* box, int target, const int* kvec, const double* amp, int nmodes, double scale);
+
+/* ---- batches: many independent periodic boxes advanced together --------
+ * All boxes of a batch share precision and device; sizes, Riemann solvers,
+ * passive counts and physics parameters may differ.  Every kernel launch of a
+ * step covers all boxes.  Each box keeps its own clock on the device and runs
+ * the reference driver loop (driver.f90:35-186) by itself: first dt, drive
+ * schedule, dt halving, COUR halving after a drive, MIN(t_end - t, dt).  One
+ * step of the whole batch is captured once into a CUDA graph and replayed.
+ * No reference counterpart (the reference advances one box per process). */
+typedef struct imhd_batch imhd_batch;
+int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** batch);
+int imhd_batch_upload(imhd_batch* batch, int box, const double* q, const double* bface, const double* qpass);
+int imhd_batch_set_force(imhd_batch* batch, int box, const double* delv);
+int imhd_batch_download(imhd_batch* batch, int box, double* q, double* bface, double* qpass);
+/* Start the clock of one box: time t0, end time t_end, number of steps, first
+ * dt (the reference uses 1e-15, driver.f90:249; dt0 <= 0 takes COUR*dx/cmax of
+ * the uploaded state), forcing on (needs edot > 0) or off. */
+int imhd_batch_schedule(imhd_batch* batch, int box, double t0, double t_end, long long steps, double dt0,
+                        int forcing);
+/* Replay the batch step `replays` times; boxes that have made their steps or
+ * reached t_end stay as they are. */
+int imhd_batch_run(imhd_batch* batch, int replays);
+/* Clock of one box: time, steps made, next dt, still running. */
+int imhd_batch_clock(imhd_batch* batch, int box, double* t, long long* steps, double* dt, int* active);
+int imhd_batch_fourier_field(imhd_batch* batch, int box, int target, const int* kvec, const double* amp, int nmodes,
+                             double scale);
+int imhd_batch_set_stream(imhd_batch* batch, void* stream);
+long long imhd_batch_launch_count(imhd_batch* batch);
+void imhd_batch_destroy(imhd_batch* batch);
+
 /* One undriven time step, like imhd_step, for callers that cannot allocate
  * device memory: hosts that own every device buffer (pool allocators,
  * OpenACC / CUDA Fortran managed arrays), code running inside a CUDA graph
@@ -163,7 +202,7 @@ int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int res
  * the host, *dt_next (host) receives COUR*dx/cmax, stream may be NULL.
  * The step's work arrays live in one 48 MiB file-scope device array held by
  * every GPU that loads the library until exit; boxes needing more
- * ((21 + npass) * nx*ny*nz * element size + 4 KiB: 64^3 in FP64, about 80^3
+ * ((21 + npass) * nx*ny*nz * element size + 56 KiB: 64^3 in FP64, about 80^3
  * in FP32 with two passives) are rejected with IMHD_E_ARG.  All calls on a
  * device share that array: calls that overlap on the GPU race.  The first
  * call on a device looks up the array's device address; make it before any

@@ -20,7 +20,10 @@ EXPORTS = (
     "imhd_default_config", "imhd_create", "imhd_upload", "imhd_download", "imhd_set_force",
     "imhd_step", "imhd_max_speed", "imhd_diagnostics", "imhd_status", "imhd_wave_speeds",
     "imhd_destroy", "imhd_last_error", "imhd_launch_count", "imhd_set_stream", "imhd_profile",
-    "imhd_stage_times", "imhd_step_static",
+    "imhd_stage_times", "imhd_step_static", "imhd_fourier_field",
+    "imhd_batch_create", "imhd_batch_upload", "imhd_batch_set_force", "imhd_batch_download", "imhd_batch_schedule",
+    "imhd_batch_run", "imhd_batch_clock", "imhd_batch_fourier_field", "imhd_batch_set_stream",
+    "imhd_batch_launch_count", "imhd_batch_destroy",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -91,6 +94,30 @@ def lib():
         L.imhd_stage_times.restype = i
         L.imhd_step_static.argtypes = [i, i, i, i, i, i, d, d, vp, vp, d, dp, vp]
         L.imhd_step_static.restype = i
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.imhd_fourier_field.argtypes = [vp, i, ip, dp, i, d]
+        L.imhd_fourier_field.restype = i
+        L.imhd_batch_create.argtypes = [ctypes.POINTER(ImhdConfig), i, ctypes.POINTER(vp)]
+        L.imhd_batch_create.restype = i
+        for name in ("imhd_batch_upload", "imhd_batch_download"):
+            getattr(L, name).argtypes = [vp, i, dp, dp, dp]
+            getattr(L, name).restype = i
+        L.imhd_batch_set_force.argtypes = [vp, i, dp]
+        L.imhd_batch_set_force.restype = i
+        L.imhd_batch_schedule.argtypes = [vp, i, d, d, ctypes.c_longlong, d, i]
+        L.imhd_batch_schedule.restype = i
+        L.imhd_batch_run.argtypes = [vp, i]
+        L.imhd_batch_run.restype = i
+        L.imhd_batch_clock.argtypes = [vp, i, dp, ctypes.POINTER(ctypes.c_longlong), dp, ip]
+        L.imhd_batch_clock.restype = i
+        L.imhd_batch_fourier_field.argtypes = [vp, i, i, ip, dp, i, d]
+        L.imhd_batch_fourier_field.restype = i
+        L.imhd_batch_set_stream.argtypes = [vp, vp]
+        L.imhd_batch_set_stream.restype = i
+        L.imhd_batch_launch_count.argtypes = [vp]
+        L.imhd_batch_launch_count.restype = ctypes.c_longlong
+        L.imhd_batch_destroy.argtypes = [vp]
+        L.imhd_batch_destroy.restype = None
         _lib = L
     return _lib
 

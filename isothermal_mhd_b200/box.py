@@ -156,6 +156,16 @@ class Box:
         ``torch.cuda.current_stream().cuda_stream``); None restores the box's own."""
         check(lib().imhd_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
 
+    def fourier_field(self, target, kvec, amp, scale):
+        """Fill from Fourier modes on the device: target "velocity" adds
+        rho * scale * v to the momentum, "force" sets the force field to scale * v
+        (v = sum_m 2 Re(amp_m exp(2 pi i k_m . x)), see imhd_fourier_field)."""
+        kv = np.ascontiguousarray(kvec, dtype=np.int32).reshape(-1, 3)
+        am = np.ascontiguousarray(amp, dtype=np.float64).reshape(-1, 6)
+        check(lib().imhd_fourier_field(self._h, {"velocity": 0, "force": 1}[target],
+                                       kv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(am), len(kv),
+                                       float(scale)))
+
     def profile(self, enable=True):
         check(lib().imhd_profile(self._h, 1 if enable else 0))
 

@@ -31,8 +31,9 @@ UNITS = {
     "imhd_f32.cu": ["--fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "imhd_capi.cu": [],
     "imhd_static.cu": [],
+    "imhd_batch.cu": [],
 }
-HEADERS = ["imhd_physics.cuh", "imhd_physics_fast.cuh", "imhd_types.cuh", "imhd_kernels.cuh", "imhd_launch.cuh"]
+HEADERS = ["imhd_physics.cuh", "imhd_physics_fast.cuh", "imhd_types.cuh", "imhd_table.h", "imhd_kernels.cuh", "imhd_launch.cuh"]
 
 
 def nvcc() -> str:

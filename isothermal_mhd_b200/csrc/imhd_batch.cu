@@ -1,0 +1,426 @@
+// imhd_batch.cu -- many independent periodic boxes advanced together.
+//
+// All boxes of a batch share one table (imhd_table.h): every kernel launch of
+// a step covers the blocks of all boxes, so small boxes no longer pay a full
+// step's launch latency each and large and small boxes fill the GPU together.
+// Each box keeps its own clock on the device (Scalars: t, dt, t_turb, steps),
+// so a step reads nothing from the host: one step of the whole batch is
+// captured once into a CUDA graph and replayed.  This is the reference's
+// driver loop (driver.f90:35-186) run per box on the device.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/imhd.h"
+#include "imhd_table.h"
+#include "imhd_types.cuh"
+
+namespace imhd {
+template <class T> cudaError_t run_step(BatchDev&, int);
+template <class T> cudaError_t prepare_launch(BatchDev&);
+template <class T> cudaError_t run_max_speed(BatchDev&);
+template <class T> cudaError_t run_diag(BatchDev&);
+template <class T> cudaError_t run_from_f64(cudaStream_t, const double*, void*, int);
+template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, int);
+template <class T> cudaError_t run_ou_field(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int,
+                                            double);
+const char* set_last_error(int code, const char* msg);
+}  // namespace imhd
+
+struct imhd_batch {
+    std::vector<imhd_config> cfg;
+    std::vector<imhd::BoxRec> rec;      // host copies of the device records
+    imhd::BatchDev b;
+    size_t esz = 8;
+    int device = 0;
+    void* pool = nullptr;
+    void* table = nullptr;
+    double* staging = nullptr;          // largest box, doubles
+    int* modes_dev = nullptr;           // scratch of the field generator
+    double* amps_dev = nullptr;
+    int modes_cap = 0;
+    cudaStream_t st = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graph_dirty = true;
+};
+
+namespace {
+
+int bfail(int code, const std::string& m) {
+    imhd::set_last_error(code, m.c_str());
+    return code;
+}
+
+#define BCK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return bfail(IMHD_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool b64(const imhd_batch* x) { return x->b.precision == 64; }
+
+const double* bhost_field(const imhd_config& c, const double* h, int f, int ng) {
+    size_t P = (size_t)(c.nx + 2 * ng) * (c.ny + 2 * ng) * (c.nz + 2 * ng);
+    return h + (size_t)f * P;
+}
+
+int bcopy(imhd_batch* x, const imhd_config& c, const void* src, void* dst, int ng, cudaMemcpyKind kind, bool padded_is_src) {
+    if (ng == 0) {
+        BCK(cudaMemcpyAsync(dst, src, (size_t)c.nx * c.ny * c.nz * 8, kind, x->st));
+        return IMHD_OK;
+    }
+    cudaMemcpy3DParms p;
+    std::memset(&p, 0, sizeof(p));
+    cudaPitchedPtr padded = make_cudaPitchedPtr(const_cast<void*>(padded_is_src ? src : dst), (size_t)(c.nx + 2 * ng) * 8,
+                                                (size_t)(c.nx + 2 * ng), (size_t)(c.ny + 2 * ng));
+    cudaPitchedPtr dense = make_cudaPitchedPtr(const_cast<void*>(padded_is_src ? dst : src), (size_t)c.nx * 8,
+                                               (size_t)c.nx, (size_t)c.ny);
+    if (padded_is_src) {
+        p.srcPtr = padded; p.srcPos = make_cudaPos((size_t)ng * 8, (size_t)ng, (size_t)ng);
+        p.dstPtr = dense; p.dstPos = make_cudaPos(0, 0, 0);
+    } else {
+        p.srcPtr = dense; p.srcPos = make_cudaPos(0, 0, 0);
+        p.dstPtr = padded; p.dstPos = make_cudaPos((size_t)ng * 8, (size_t)ng, (size_t)ng);
+    }
+    p.extent = make_cudaExtent((size_t)c.nx * 8, (size_t)c.ny, (size_t)c.nz);
+    p.kind = kind;
+    BCK(cudaMemcpy3DAsync(&p, x->st));
+    return IMHD_OK;
+}
+
+int bupload_field(imhd_batch* x, int box, const double* h, int ng, void* dst) {
+    const imhd_config& c = x->cfg[box];
+    if (b64(x)) return bcopy(x, c, h, dst, ng, cudaMemcpyHostToDevice, true);
+    int rc = bcopy(x, c, h, x->staging, ng, cudaMemcpyHostToDevice, true);
+    if (rc) return rc;
+    BCK(imhd::run_from_f64<float>(x->st, x->staging, dst, x->rec[box].n));
+    x->b.launches += 1;
+    return IMHD_OK;
+}
+
+int bdownload_field(imhd_batch* x, int box, const void* src, double* h, int ng) {
+    const imhd_config& c = x->cfg[box];
+    if (b64(x)) {
+        int rc = bcopy(x, c, src, h, ng, cudaMemcpyDeviceToHost, false);
+        if (rc) return rc;
+    } else {
+        BCK(imhd::run_to_f64<float>(x->st, src, x->staging, x->rec[box].n));
+        x->b.launches += 1;
+        int rc = bcopy(x, c, x->staging, h, ng, cudaMemcpyDeviceToHost, false);
+        if (rc) return rc;
+    }
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+void bghost_fill(const imhd_config& c, double* h, int ng) {
+    if (ng == 0) return;
+    long Px = c.nx + 2 * ng, Py = c.ny + 2 * ng, Pz = c.nz + 2 * ng;
+    auto wrap = [](long i, long n) { i %= n; return i < 0 ? i + n : i; };
+    for (long k = 0; k < Pz; ++k)
+        for (long j = 0; j < Py; ++j)
+            for (long i = 0; i < Px; ++i) {
+                bool in = i >= ng && i < ng + c.nx && j >= ng && j < ng + c.ny && k >= ng && k < ng + c.nz;
+                if (in) continue;
+                long ii = wrap(i - ng, c.nx) + ng, jj = wrap(j - ng, c.ny) + ng, kk = wrap(k - ng, c.nz) + ng;
+                h[i + Px * (j + Py * k)] = h[ii + Px * (jj + Py * kk)];
+            }
+}
+
+int read_scalars(imhd_batch* x, int box, imhd::Scalars& s) {
+    BCK(cudaMemcpyAsync(&s, x->rec[box].sc, sizeof(s), cudaMemcpyDeviceToHost, x->st));
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+int write_scalars(imhd_batch* x, int box, const imhd::Scalars& s) {
+    BCK(cudaMemcpyAsync(x->rec[box].sc, &s, sizeof(s), cudaMemcpyHostToDevice, x->st));
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+bool check_box(imhd_batch* x, int box) { return x && box >= 0 && box < (int)x->rec.size(); }
+
+}  // namespace
+
+extern "C" {
+
+int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
+    if (!cfgs || !out || nbox < 1) return bfail(IMHD_E_ARG, "need at least one box configuration");
+    *out = nullptr;
+    int prec = cfgs[0].precision, dev = cfgs[0].device;
+    for (int i = 0; i < nbox; ++i) {
+        const imhd_config& c = cfgs[i];
+        if (c.precision != prec || c.device != dev) return bfail(IMHD_E_ARG, "all boxes of a batch share precision and device");
+        if (c.nx < 4 || c.ny < 4 || c.nz < 4) return bfail(IMHD_E_ARG, "every edge needs at least 4 cells");
+        if ((double)c.nx * c.ny * c.nz >= 2147483647.0) return bfail(IMHD_E_ARG, "box too large");
+        if (c.precision != 32 && c.precision != 64) return bfail(IMHD_E_ARG, "precision must be 32 or 64");
+        if (c.riemann < 1 || c.riemann > 3) return bfail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
+        if (c.recon != IMHD_PLM) return bfail(IMHD_E_ARG, "only IMHD_PLM reconstruction is implemented");
+        if (c.npass < 0 || c.npass > imhd::kMaxPass) return bfail(IMHD_E_ARG, "npass must be in 0..8");
+        if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return bfail(IMHD_E_ARG, "sound_speed and cour must be positive");
+    }
+    int ndev = 0;
+    BCK(cudaGetDeviceCount(&ndev));
+    if (dev < 0 || dev >= ndev) return bfail(IMHD_E_ARG, "no such CUDA device");
+    BCK(cudaSetDevice(dev));
+    imhd_batch* x = new imhd_batch();
+    x->cfg.assign(cfgs, cfgs + nbox);
+    x->esz = prec == 64 ? 8 : 4;
+    x->device = dev;
+    x->b.precision = prec;
+    x->rec.resize(nbox);
+    size_t total = 0, maxn = 0;
+    bool forcing = false;
+    for (int i = 0; i < nbox; ++i) {
+        const imhd_config& c = cfgs[i];
+        imhd::init_rec(x->rec[i], c.nx, c.ny, c.nz, c.npass, c.riemann, c.sound_speed, c.cour, c.edot, c.dt_turb);
+        total += imhd::box_bytes(x->rec[i], x->esz, true);
+        if ((size_t)x->rec[i].n > maxn) maxn = x->rec[i].n;
+        forcing = forcing || c.edot > 0.0;
+    }
+    std::vector<int> prefix;
+    if (!imhd::build_prefix(x->rec, x->esz, prefix, x->b)) { delete x; return bfail(IMHD_E_ARG, "batch too large for one launch"); }
+    std::vector<std::vector<int>> b2b;
+    imhd::build_blk2box(prefix, nbox, x->b, b2b);
+    size_t tab = imhd::align256(sizeof(imhd::BoxRec) * nbox) + imhd::align256(prefix.size() * sizeof(int));
+    for (int k = 0; k < imhd::kKinds; ++k) tab += imhd::align256(b2b[k].size() * sizeof(int) + 4);
+    bool ok = cudaStreamCreateWithFlags(&x->st, cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaMalloc(&x->pool, total) == cudaSuccess;
+    ok = ok && cudaMalloc(&x->table, tab) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&x->staging, maxn * 8) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        imhd_batch_destroy(x);
+        return bfail(IMHD_E_NOMEM, "device allocation of the batch failed (" + std::to_string(total) + " bytes)");
+    }
+    x->b.st = x->st;
+    unsigned char* p = (unsigned char*)x->pool;
+    for (int i = 0; i < nbox; ++i) {
+        imhd::carve_box(x->rec[i], p, x->esz, true);
+        p += imhd::box_bytes(x->rec[i], x->esz, true);
+        x->rec[i].active = 0;            // until scheduled
+    }
+    BCK(cudaMemsetAsync(x->pool, 0, total, x->st));
+    for (int i = 0; i < nbox; ++i) {
+        imhd::Scalars init;
+        std::memset(&init, 0, sizeof(init));
+        BCK(cudaMemcpyAsync(x->rec[i].sc, &init, sizeof(init), cudaMemcpyHostToDevice, x->st));
+    }
+    BCK(cudaMemcpyAsync(x->table, x->rec.data(), sizeof(imhd::BoxRec) * nbox, cudaMemcpyHostToDevice, x->st));
+    size_t off = imhd::align256(sizeof(imhd::BoxRec) * nbox);
+    BCK(cudaMemcpyAsync((char*)x->table + off, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice, x->st));
+    x->b.a.boxes = (imhd::BoxRec*)x->table;
+    x->b.a.prefix = (const int*)((char*)x->table + off);
+    off += imhd::align256(prefix.size() * sizeof(int));
+    for (int k = 0; k < imhd::kKinds; ++k) {
+        if (!b2b[k].empty())
+            BCK(cudaMemcpyAsync((char*)x->table + off, b2b[k].data(), b2b[k].size() * sizeof(int), cudaMemcpyHostToDevice,
+                                x->st));
+        x->b.a.blk2box[k] = (const int*)((char*)x->table + off);
+        off += imhd::align256(b2b[k].size() * sizeof(int) + 4);
+    }
+    BCK(cudaStreamSynchronize(x->st));
+    x->b.a.use_one = 0;
+    x->b.drive_mode = forcing ? 2 : 0;
+    *out = x;
+    return IMHD_OK;
+}
+
+void imhd_batch_destroy(imhd_batch* x) {
+    if (!x) return;
+    cudaSetDevice(x->device);
+    if (x->st) cudaStreamSynchronize(x->st);
+    if (x->exec) cudaGraphExecDestroy(x->exec);
+    if (x->graph) cudaGraphDestroy(x->graph);
+    void* ptrs[] = {x->pool, x->table, x->staging, x->modes_dev, x->amps_dev};
+    for (void* q : ptrs)
+        if (q) cudaFree(q);
+    if (x->st) cudaStreamDestroy(x->st);
+    delete x;
+}
+
+int imhd_batch_upload(imhd_batch* x, int box, const double* q, const double* bface, const double* qpass) {
+    if (!check_box(x, box) || !q || !bface) return bfail(IMHD_E_ARG, "bad box index or null array");
+    const imhd_config& c = x->cfg[box];
+    if (c.npass > 0 && !qpass) return bfail(IMHD_E_ARG, "qpass is NULL but npass > 0");
+    BCK(cudaSetDevice(x->device));
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    imhd::BoxRec& r = x->rec[box];
+    size_t fb = (size_t)r.n * x->esz;
+    char* S = (char*)r.S[s.cur];
+    for (int f = 0; f < 7; ++f)
+        if ((rc = bupload_field(x, box, bhost_field(c, q, f, c.ng), c.ng, S + f * fb))) return rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = bupload_field(x, box, bhost_field(c, bface, f, c.ng), c.ng, S + (7 + f) * fb))) return rc;
+    for (int f = 0; f < c.npass; ++f)
+        if ((rc = bupload_field(x, box, bhost_field(c, qpass, f, c.ng_pass), c.ng_pass, S + (10 + f) * fb))) return rc;
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+int imhd_batch_set_force(imhd_batch* x, int box, const double* delv) {
+    if (!check_box(x, box) || !delv) return bfail(IMHD_E_ARG, "bad box index or null array");
+    BCK(cudaSetDevice(x->device));
+    const imhd_config& c = x->cfg[box];
+    imhd::BoxRec& r = x->rec[box];
+    size_t fb = (size_t)r.n * x->esz;
+    int rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = bupload_field(x, box, bhost_field(c, delv, f, c.ng), c.ng, (char*)r.delv + f * fb))) return rc;
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+int imhd_batch_download(imhd_batch* x, int box, double* q, double* bface, double* qpass) {
+    if (!check_box(x, box)) return bfail(IMHD_E_ARG, "bad box index");
+    BCK(cudaSetDevice(x->device));
+    const imhd_config& c = x->cfg[box];
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    imhd::BoxRec& r = x->rec[box];
+    size_t fb = (size_t)r.n * x->esz;
+    const char* S = (const char*)r.S[s.cur];
+    if (q)
+        for (int f = 0; f < 7; ++f)
+            if ((rc = bdownload_field(x, box, S + f * fb, (double*)bhost_field(c, q, f, c.ng), c.ng))) return rc;
+    if (bface)
+        for (int f = 0; f < 3; ++f)
+            if ((rc = bdownload_field(x, box, S + (7 + f) * fb, (double*)bhost_field(c, bface, f, c.ng), c.ng))) return rc;
+    if (qpass)
+        for (int f = 0; f < c.npass; ++f)
+            if ((rc = bdownload_field(x, box, S + (10 + f) * fb, (double*)bhost_field(c, qpass, f, c.ng_pass), c.ng_pass)))
+                return rc;
+    if (q) for (int f = 0; f < 7; ++f) bghost_fill(c, (double*)bhost_field(c, q, f, c.ng), c.ng);
+    if (bface) for (int f = 0; f < 3; ++f) bghost_fill(c, (double*)bhost_field(c, bface, f, c.ng), c.ng);
+    if (qpass) for (int f = 0; f < c.npass; ++f) bghost_fill(c, (double*)bhost_field(c, qpass, f, c.ng_pass), c.ng_pass);
+    return IMHD_OK;
+}
+
+int imhd_batch_schedule(imhd_batch* x, int box, double t0, double t_end, long long steps, double dt0, int forcing) {
+    if (!check_box(x, box)) return bfail(IMHD_E_ARG, "bad box index");
+    if (steps < 0) return bfail(IMHD_E_ARG, "steps must be >= 0");
+    if (forcing && x->b.drive_mode == 0) return bfail(IMHD_E_STATE, "forcing needs edot > 0 in the box configuration");
+    BCK(cudaSetDevice(x->device));
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    const imhd::BoxRec& r = x->rec[box];
+    if (!(dt0 > 0.0)) {
+        // COUR*dx/cmax of the uploaded state (get_max_speed_vanleer without smax)
+        for (int k = 0; k < imhd::kSlots; ++k) s.cfl_slots[k] = 0ull;
+        if ((rc = write_scalars(x, box, s))) return rc;
+        BCK(b64(x) ? imhd::run_max_speed<double>(x->b) : imhd::run_max_speed<float>(x->b));
+        if ((rc = read_scalars(x, box, s))) return rc;
+        double m = 0.0;
+        for (int k = 0; k < imhd::kSlots; ++k) {
+            double v;
+            std::memcpy(&v, &s.cfl_slots[k], 8);
+            if (v != v || v > m) m = v;
+        }
+        if (!(m > 0.0)) return bfail(IMHD_E_PHYSICS, "zero max speed encountered");
+        dt0 = r.cour * r.dx / m;
+    }
+    s.t = t0;
+    s.t_end = t_end;
+    s.dt = (t_end - t0 < dt0) ? t_end - t0 : dt0;
+    s.t_turb = t0 + r.dt_turb;          // driver.f90:342
+    s.dt_turb_sched = r.dt_turb;
+    s.steps_done = 0;
+    s.steps_target = steps;
+    s.forcing = forcing ? 1 : 0;
+    s.active = (steps > 0 && t0 < t_end) ? 1 : 0;
+    s.drive = 0;
+    for (int k = 0; k < imhd::kSlots; ++k) s.smax_slots[k] = s.cmax_slots[k] = s.dvmax_slots[k] = 0ull;
+    if ((rc = write_scalars(x, box, s))) return rc;
+    // the device table holds the running flag the kernels read
+    imhd::BoxRec* dev = (imhd::BoxRec*)x->table + box;
+    BCK(cudaMemcpyAsync(&dev->active, &s.active, sizeof(int), cudaMemcpyHostToDevice, x->st));
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+int imhd_batch_run(imhd_batch* x, int replays) {
+    if (!x || replays < 0) return bfail(IMHD_E_ARG, "bad argument");
+    BCK(cudaSetDevice(x->device));
+    if (x->graph_dirty) {
+        BCK(b64(x) ? imhd::prepare_launch<double>(x->b) : imhd::prepare_launch<float>(x->b));
+        if (x->exec) { cudaGraphExecDestroy(x->exec); x->exec = nullptr; }
+        if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
+        BCK(cudaStreamBeginCapture(x->st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = b64(x) ? imhd::run_step<double>(x->b, 1) : imhd::run_step<float>(x->b, 1);
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(x->st, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return bfail(IMHD_E_CUDA, std::string("graph capture of the batch step failed: ") +
+                                          cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        x->graph = g;
+        BCK(cudaGraphInstantiate(&x->exec, x->graph, 0));
+        x->graph_dirty = false;
+    }
+    for (int r = 0; r < replays; ++r) BCK(cudaGraphLaunch(x->exec, x->st));
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+int imhd_batch_clock(imhd_batch* x, int box, double* t, long long* steps, double* dt, int* active) {
+    if (!check_box(x, box)) return bfail(IMHD_E_ARG, "bad box index");
+    BCK(cudaSetDevice(x->device));
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    if (t) *t = s.t;
+    if (steps) *steps = s.steps_done;
+    if (dt) *dt = s.dt;
+    if (active) *active = s.active;
+    if (s.status & (IMHD_S_ZERO_SPEED | IMHD_S_FORCE)) return bfail(IMHD_E_PHYSICS, "box stopped on a physics error");
+    return IMHD_OK;
+}
+
+int imhd_batch_set_stream(imhd_batch* x, void* stream) {
+    if (!x) return bfail(IMHD_E_ARG, "null argument");
+    BCK(cudaSetDevice(x->device));
+    BCK(cudaStreamSynchronize(x->st));
+    x->b.st = stream ? (cudaStream_t)stream : x->st;
+    x->st = x->b.st;
+    return IMHD_OK;
+}
+
+long long imhd_batch_launch_count(imhd_batch* x) { return x ? x->b.launches : 0; }
+
+// Fill one box from a sum of Fourier modes (see imhd_ou_field in imhd.h).
+int imhd_batch_fourier_field(imhd_batch* x, int box, int target, const int* kvec, const double* amp, int nmodes,
+                             double scale) {
+    if (!check_box(x, box) || nmodes < 0 || (nmodes > 0 && (!kvec || !amp))) return bfail(IMHD_E_ARG, "bad argument");
+    if (target != 0 && target != 1) return bfail(IMHD_E_ARG, "target must be 0 (velocity) or 1 (force)");
+    BCK(cudaSetDevice(x->device));
+    if (nmodes > x->modes_cap) {
+        if (x->modes_dev) cudaFree(x->modes_dev);
+        if (x->amps_dev) cudaFree(x->amps_dev);
+        x->modes_dev = nullptr; x->amps_dev = nullptr;
+        BCK(cudaMalloc((void**)&x->modes_dev, (size_t)nmodes * 3 * sizeof(int)));
+        BCK(cudaMalloc((void**)&x->amps_dev, (size_t)nmodes * 6 * sizeof(double)));
+        x->modes_cap = nmodes;
+    }
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    if (nmodes) {
+        BCK(cudaMemcpyAsync(x->modes_dev, kvec, (size_t)nmodes * 3 * sizeof(int), cudaMemcpyHostToDevice, x->st));
+        BCK(cudaMemcpyAsync(x->amps_dev, amp, (size_t)nmodes * 6 * sizeof(double), cudaMemcpyHostToDevice, x->st));
+    }
+    BCK(b64(x) ? imhd::run_ou_field<double>(x->st, x->rec[box], s.cur, target, x->modes_dev, x->amps_dev, nmodes, scale)
+               : imhd::run_ou_field<float>(x->st, x->rec[box], s.cur, target, x->modes_dev, x->amps_dev, nmodes, scale));
+    x->b.launches += 1;
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+}  // extern "C"

@@ -9,20 +9,27 @@
 #include <vector>
 
 #include "../../include/imhd.h"
+#include "imhd_table.h"
 #include "imhd_types.cuh"
 
 namespace imhd {
-template <class T> cudaError_t run_step(BoxDev&, int);
-template <class T> cudaError_t run_max_speed(BoxDev&);
-template <class T> cudaError_t run_diag(BoxDev&);
-template <class T> cudaError_t run_from_f64(BoxDev&, const double*, void*);
-template <class T> cudaError_t run_to_f64(BoxDev&, const void*, double*);
+template <class T> cudaError_t run_step(BatchDev&, int);
+template <class T> cudaError_t run_max_speed(BatchDev&);
+template <class T> cudaError_t run_diag(BatchDev&);
+template <class T> cudaError_t run_from_f64(cudaStream_t, const double*, void*, int);
+template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, int);
+template <class T> cudaError_t run_ou_field(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int,
+                                            double);
 }  // namespace imhd
 
 struct imhd_box {
     imhd_config cfg;
-    imhd::BoxDev b;
+    imhd::BoxRec rec;            // host copy of the device record
+    imhd::BatchDev b;            // a table of one box
     size_t esz = 8;
+    int cur = 0;                 // host mirror of Scalars::cur
+    void* pool = nullptr;        // all buffers of the box
+    void* table = nullptr;       // device BoxRec + prefix
     double* staging = nullptr;   // N doubles on the device
     double* hio = nullptr;       // pinned host scalars
     bool have_force = false;
@@ -48,11 +55,37 @@ int fail(int code, const std::string& msg) {
 
 bool is64(const imhd_box* x) { return x->cfg.precision == 64; }
 
-cudaError_t step_dispatch(imhd_box* x, int drive) {
-    return is64(x) ? imhd::run_step<double>(x->b, drive) : imhd::run_step<float>(x->b, drive);
+// The box travels by value in the launch parameters, current state first.
+void set_one(imhd_box* x) {
+    x->b.a.use_one = 1;
+    x->b.a.one = x->rec;
+    x->b.a.one.S[0] = x->rec.S[x->cur];
+    x->b.a.one.S[1] = x->rec.S[x->cur ^ 1];
+    x->b.a.one.active = 1;
 }
 
-void* field_ptr(imhd_box* x, void* base, int f) { return (char*)base + (size_t)f * (size_t)x->b.dm.n * x->esz; }
+cudaError_t step_dispatch(imhd_box* x) {
+    set_one(x);
+    return is64(x) ? imhd::run_step<double>(x->b, 0) : imhd::run_step<float>(x->b, 0);
+}
+
+void* field_ptr(imhd_box* x, void* base, int f) { return (char*)base + (size_t)f * (size_t)x->rec.n * x->esz; }
+void* cur_state(imhd_box* x) { return x->rec.S[x->cur]; }
+
+// (Re)write the device table of the box: its record and block prefixes.
+int upload_table(imhd_box* x) {
+    std::vector<imhd::BoxRec> recs(1, x->rec);
+    std::vector<int> prefix;
+    if (!imhd::build_prefix(recs, x->esz, prefix, x->b)) return fail(IMHD_E_ARG, "box too large for one launch");
+    CK(cudaMemcpyAsync(x->table, &x->rec, sizeof(imhd::BoxRec), cudaMemcpyHostToDevice, x->b.st));
+    CK(cudaMemcpyAsync((char*)x->table + imhd::align256(sizeof(imhd::BoxRec)), prefix.data(), prefix.size() * sizeof(int),
+                       cudaMemcpyHostToDevice, x->b.st));
+    CK(cudaStreamSynchronize(x->b.st));
+    x->b.a.boxes = (imhd::BoxRec*)x->table;
+    x->b.a.prefix = (const int*)((char*)x->table + imhd::align256(sizeof(imhd::BoxRec)));
+    set_one(x);
+    return IMHD_OK;
+}
 
 // host field f of a Fortran array a(1-ng:n+ng, ..., nf)
 const double* host_field(const imhd_box* x, const double* h, int f, int ng) {
@@ -64,7 +97,7 @@ const double* host_field(const imhd_box* x, const double* h, int f, int ng) {
 int copy_in_f64(imhd_box* x, const double* hfield, int ng, double* dst) {
     const imhd_config& c = x->cfg;
     if (ng == 0) {
-        CK(cudaMemcpyAsync(dst, hfield, (size_t)x->b.dm.n * 8, cudaMemcpyHostToDevice, x->b.st));
+        CK(cudaMemcpyAsync(dst, hfield, (size_t)x->rec.n * 8, cudaMemcpyHostToDevice, x->b.st));
         return IMHD_OK;
     }
     cudaMemcpy3DParms p;
@@ -82,7 +115,7 @@ int copy_in_f64(imhd_box* x, const double* hfield, int ng, double* dst) {
 int copy_out_f64(imhd_box* x, const double* src, double* hfield, int ng) {
     const imhd_config& c = x->cfg;
     if (ng == 0) {
-        CK(cudaMemcpyAsync(hfield, src, (size_t)x->b.dm.n * 8, cudaMemcpyDeviceToHost, x->b.st));
+        CK(cudaMemcpyAsync(hfield, src, (size_t)x->rec.n * 8, cudaMemcpyDeviceToHost, x->b.st));
         return IMHD_OK;
     }
     cudaMemcpy3DParms p;
@@ -102,13 +135,15 @@ int upload_field(imhd_box* x, const double* hfield, int ng, void* dst) {
     if (is64(x)) return copy_in_f64(x, hfield, ng, (double*)dst);
     int rc = copy_in_f64(x, hfield, ng, x->staging);
     if (rc) return rc;
-    CK(imhd::run_from_f64<float>(x->b, x->staging, dst));
+    CK(imhd::run_from_f64<float>(x->b.st, x->staging, dst, x->rec.n));
+    x->b.launches += 1;
     return IMHD_OK;
 }
 
 int download_field(imhd_box* x, const void* src, double* hfield, int ng) {
     if (is64(x)) return copy_out_f64(x, (const double*)src, hfield, ng);
-    CK(imhd::run_to_f64<float>(x->b, src, x->staging));
+    CK(imhd::run_to_f64<float>(x->b.st, src, x->staging, x->rec.n));
+    x->b.launches += 1;
     return copy_out_f64(x, x->staging, hfield, ng);
 }
 
@@ -141,7 +176,7 @@ int sync_and_check(imhd_box* x) {
 
 // Fold the events of the last step into the per-stage accumulators.
 int accumulate_stage_times(imhd_box* x) {
-    imhd::BoxDev& b = x->b;
+    imhd::BatchDev& b = x->b;
     if (!b.prof) return IMHD_OK;
     for (int s = 0; s < imhd::kStages; ++s) {
         if (!(b.prof_mask & (1u << s))) continue;
@@ -192,6 +227,7 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     const imhd_config& c = *cfg;
     if (c.nx < 4 || c.ny < 4 || c.nz < 4) return fail(IMHD_E_ARG, "every edge needs at least 4 cells");
     if ((double)c.nx * c.ny * c.nz >= 2147483647.0) return fail(IMHD_E_ARG, "box too large (nx*ny*nz must be < 2^31)");
+    if (c.ny > 65535 || c.nz > 65535) return fail(IMHD_E_ARG, "ny and nz must be <= 65535");
     if (c.precision != 32 && c.precision != 64) return fail(IMHD_E_ARG, "precision must be 32 or 64");
     if (c.riemann < 1 || c.riemann > 3) return fail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
     if (c.recon != IMHD_PLM) return fail(IMHD_E_ARG, "only IMHD_PLM reconstruction is implemented");
@@ -206,41 +242,30 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     imhd_box* x = new imhd_box();
     x->cfg = c;
     x->esz = c.precision == 64 ? 8 : 4;
-    imhd::BoxDev& b = x->b;
-    b.dm.nx = c.nx; b.dm.ny = c.ny; b.dm.nz = c.nz; b.dm.n = c.nx * c.ny * c.nz;
-    b.riemann = c.riemann;
-    b.npass = c.npass;
-    b.cs = c.sound_speed;
-    int nmax = c.nx > c.ny ? c.nx : c.ny;
-    nmax = nmax > c.nz ? nmax : c.nz;
-    b.dx = 1.0 / (double)nmax;                  // vanleer_mod.f90:177, driver.f90:254
-    b.cour = c.cour;
-    b.edot = c.edot;
-    b.dt_turb = c.dt_turb;
-    int pmax = c.ny * c.nz;
-    if (c.nx * c.nz > pmax) pmax = c.nx * c.nz;
-    if (c.nx * c.ny > pmax) pmax = c.nx * c.ny;
-    b.plane_stride = pmax;
-    b.nred = 1024;
-    size_t N = (size_t)b.dm.n;
-    size_t nf = 10 + (size_t)c.npass;
-    auto alloc = [&](void** p, size_t bytes) -> bool { return cudaMalloc(p, bytes) == cudaSuccess; };
+    imhd::init_rec(x->rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.sound_speed, c.cour, c.edot, c.dt_turb);
+    imhd::BatchDev& b = x->b;
+    b.precision = c.precision;
+    size_t N = (size_t)x->rec.n;
+    size_t table_bytes = imhd::align256(sizeof(imhd::BoxRec)) + (size_t)imhd::kKinds * 2 * sizeof(int);
     bool ok = cudaStreamCreateWithFlags(&b.st, cudaStreamNonBlocking) == cudaSuccess;
     x->own_stream = b.st;
-    ok = ok && alloc(&b.A, nf * N * x->esz) && alloc(&b.B, nf * N * x->esz) && alloc(&b.F, 18 * N * x->esz) &&
-         alloc(&b.E, 3 * N * x->esz) && alloc((void**)&b.partials, (size_t)b.nred * 6 * 8) &&
-         alloc((void**)&b.sc, sizeof(imhd::Scalars)) && alloc((void**)&x->staging, N * 8);
-    if (ok && c.npass > 0) ok = alloc(&b.SH, (size_t)c.npass * N * x->esz) && alloc(&b.mbnd, 6 * (size_t)pmax * x->esz);
-    if (ok) ok = cudaMallocHost((void**)&x->hio, 64 * sizeof(double)) == cudaSuccess;
+    ok = ok && cudaMalloc(&x->pool, imhd::box_bytes(x->rec, x->esz, false)) == cudaSuccess;
+    ok = ok && cudaMalloc(&x->table, table_bytes) == cudaSuccess;
+    ok = ok && cudaMalloc((void**)&x->staging, N * 8) == cudaSuccess;
+    ok = ok && cudaMallocHost((void**)&x->hio, 64 * sizeof(double)) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         imhd_destroy(x);
         return fail(IMHD_E_NOMEM, "device allocation failed");
     }
-    cudaMemsetAsync(b.sc, 0, sizeof(imhd::Scalars), b.st);
-    cudaMemsetAsync(b.A, 0, nf * N * x->esz, b.st);
-    cudaMemsetAsync(b.B, 0, nf * N * x->esz, b.st);
-    int rc = sync_and_check(x);
+    imhd::carve_box(x->rec, (unsigned char*)x->pool, x->esz, false);
+    cudaMemsetAsync(x->pool, 0, imhd::box_bytes(x->rec, x->esz, false), b.st);
+    imhd::Scalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.active = 1;
+    CK(cudaMemcpyAsync(x->rec.sc, &init, sizeof(init), cudaMemcpyHostToDevice, b.st));
+    int rc = upload_table(x);
+    if (!rc) rc = sync_and_check(x);
     if (rc) { imhd_destroy(x); return rc; }
     *out = x;
     return IMHD_OK;
@@ -251,7 +276,7 @@ void imhd_destroy(imhd_box* x) {
     cudaSetDevice(x->cfg.device);
     if (x->b.st) cudaStreamSynchronize(x->b.st);
     if (x->own_stream) cudaStreamSynchronize(x->own_stream);
-    void* ptrs[] = {x->b.A, x->b.B, x->b.F, x->b.E, x->b.SH, x->b.delv, x->b.mbnd, x->b.partials, x->b.sc, x->staging};
+    void* ptrs[] = {x->pool, x->table, x->rec.delv, x->staging};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (x->hio) cudaFreeHost(x->hio);
@@ -267,11 +292,11 @@ int imhd_upload(imhd_box* x, const double* q, const double* bface, const double*
     CK(cudaSetDevice(x->cfg.device));
     int rc;
     for (int f = 0; f < 7; ++f)
-        if ((rc = upload_field(x, host_field(x, q, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.A, f)))) return rc;
+        if ((rc = upload_field(x, host_field(x, q, f, x->cfg.ng), x->cfg.ng, field_ptr(x, cur_state(x), f)))) return rc;
     for (int f = 0; f < 3; ++f)
-        if ((rc = upload_field(x, host_field(x, bface, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.A, 7 + f)))) return rc;
+        if ((rc = upload_field(x, host_field(x, bface, f, x->cfg.ng), x->cfg.ng, field_ptr(x, cur_state(x), 7 + f)))) return rc;
     for (int f = 0; f < x->cfg.npass; ++f)
-        if ((rc = upload_field(x, host_field(x, qpass, f, x->cfg.ng_pass), x->cfg.ng_pass, field_ptr(x, x->b.A, 10 + f))))
+        if ((rc = upload_field(x, host_field(x, qpass, f, x->cfg.ng_pass), x->cfg.ng_pass, field_ptr(x, cur_state(x), 10 + f))))
             return rc;
     return sync_and_check(x);
 }
@@ -285,17 +310,17 @@ int imhd_download(imhd_box* x, double* q, double* bface, double* qpass) {
     // completed (stream-ordered) before the next conversion overwrites it
     if (q)
         for (int f = 0; f < 7; ++f) {
-            if ((rc = download_field(x, field_ptr(x, x->b.A, f), (double*)host_field(x, q, f, c.ng), c.ng))) return rc;
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), f), (double*)host_field(x, q, f, c.ng), c.ng))) return rc;
             if ((rc = sync_and_check(x))) return rc;
         }
     if (bface)
         for (int f = 0; f < 3; ++f) {
-            if ((rc = download_field(x, field_ptr(x, x->b.A, 7 + f), (double*)host_field(x, bface, f, c.ng), c.ng))) return rc;
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), 7 + f), (double*)host_field(x, bface, f, c.ng), c.ng))) return rc;
             if ((rc = sync_and_check(x))) return rc;
         }
     if (qpass && c.npass > 0)
         for (int f = 0; f < c.npass; ++f) {
-            if ((rc = download_field(x, field_ptr(x, x->b.A, 10 + f), (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass)))
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), 10 + f), (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass)))
                 return rc;
             if ((rc = sync_and_check(x))) return rc;
         }
@@ -308,15 +333,16 @@ int imhd_download(imhd_box* x, double* q, double* bface, double* qpass) {
 int imhd_set_force(imhd_box* x, const double* delv) {
     if (!x || !delv) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
-    if (!x->b.delv) {
-        if (cudaMalloc(&x->b.delv, 3 * (size_t)x->b.dm.n * x->esz) != cudaSuccess) {
+    int rc;
+    if (!x->rec.delv) {
+        if (cudaMalloc(&x->rec.delv, 3 * (size_t)x->rec.n * x->esz) != cudaSuccess) {
             cudaGetLastError();
             return fail(IMHD_E_NOMEM, "device allocation of the force field failed");
         }
+        if ((rc = upload_table(x))) return rc;
     }
-    int rc;
     for (int f = 0; f < 3; ++f) {
-        if ((rc = upload_field(x, host_field(x, delv, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->b.delv, f)))) return rc;
+        if ((rc = upload_field(x, host_field(x, delv, f, x->cfg.ng), x->cfg.ng, field_ptr(x, x->rec.delv, f)))) return rc;
         if ((rc = sync_and_check(x))) return rc;
     }
     x->have_force = true;
@@ -328,12 +354,17 @@ int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
     if (!(dt > 0.0)) return fail(IMHD_E_ARG, "dt must be positive");
     if (drive_next && !x->have_force) return fail(IMHD_E_STATE, "drive step requested before imhd_set_force");
     CK(cudaSetDevice(x->cfg.device));
+    imhd::Scalars* sc = x->rec.sc;
     x->hio[0] = dt;
-    CK(cudaMemcpyAsync(&x->b.sc->dt, x->hio, sizeof(double), cudaMemcpyHostToDevice, x->b.st));
-    CK(step_dispatch(x, drive_next ? 1 : 0));
-    std::swap(x->b.A, x->b.B);
-    CK(cudaMemcpyAsync(x->hio + 1, &x->b.sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
-    CK(cudaMemcpyAsync((unsigned*)(x->hio + 2), &x->b.sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, x->b.st));
+    int drive = drive_next ? 1 : 0;
+    std::memcpy(x->hio + 4, &drive, sizeof(int));
+    CK(cudaMemcpyAsync(&sc->dt, x->hio, sizeof(double), cudaMemcpyHostToDevice, x->b.st));
+    CK(cudaMemcpyAsync(&sc->drive, x->hio + 4, sizeof(int), cudaMemcpyHostToDevice, x->b.st));
+    x->b.drive_mode = drive;
+    CK(step_dispatch(x));
+    x->cur ^= 1;
+    CK(cudaMemcpyAsync(x->hio + 1, &sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync((unsigned*)(x->hio + 2), &sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
     if ((rc = accumulate_stage_times(x))) return rc;
@@ -347,9 +378,11 @@ int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
 int imhd_max_speed(imhd_box* x, double* cmax) {
     if (!x || !cmax) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
+    CK(cudaMemsetAsync(x->rec.sc->cfl_slots, 0, sizeof(x->rec.sc->cfl_slots), x->b.st));
+    set_one(x);
     CK(is64(x) ? imhd::run_max_speed<double>(x->b) : imhd::run_max_speed<float>(x->b));
     unsigned long long slots[imhd::kSlots];
-    CK(cudaMemcpyAsync(slots, x->b.sc->cfl_slots, sizeof(slots), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync(slots, x->rec.sc->cfl_slots, sizeof(slots), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
     double m = 0.0;
@@ -365,8 +398,9 @@ int imhd_max_speed(imhd_box* x, double* cmax) {
 int imhd_diagnostics(imhd_box* x, double out[6]) {
     if (!x || !out) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
+    set_one(x);
     CK(is64(x) ? imhd::run_diag<double>(x->b) : imhd::run_diag<float>(x->b));
-    CK(cudaMemcpyAsync(x->hio + 8, &x->b.sc->diag[0], 6 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync(x->hio + 8, &x->rec.sc->diag[0], 6 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
     for (int q = 0; q < 6; ++q) out[q] = x->hio[8 + q];
@@ -377,7 +411,7 @@ int imhd_status(imhd_box* x, unsigned* flags, long long* floor_hits, int reset) 
     if (!x) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
     imhd::Scalars s;
-    CK(cudaMemcpyAsync(&s, x->b.sc, sizeof(s), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync(&s, x->rec.sc, sizeof(s), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
     unsigned f = s.status;
@@ -385,8 +419,8 @@ int imhd_status(imhd_box* x, unsigned* flags, long long* floor_hits, int reset) 
     if (flags) *flags = f;
     if (floor_hits) *floor_hits = (long long)s.floor_hits;
     if (reset) {
-        CK(cudaMemsetAsync(&x->b.sc->status, 0, sizeof(unsigned), x->b.st));
-        CK(cudaMemsetAsync(&x->b.sc->floor_hits, 0, sizeof(unsigned long long), x->b.st));
+        CK(cudaMemsetAsync(&x->rec.sc->status, 0, sizeof(unsigned), x->b.st));
+        CK(cudaMemsetAsync(&x->rec.sc->floor_hits, 0, sizeof(unsigned long long), x->b.st));
         return sync_and_check(x);
     }
     return IMHD_OK;
@@ -395,7 +429,7 @@ int imhd_status(imhd_box* x, unsigned* flags, long long* floor_hits, int reset) 
 int imhd_wave_speeds(imhd_box* x, double* smax, double* delv_max) {
     if (!x) return fail(IMHD_E_ARG, "null argument");
     CK(cudaSetDevice(x->cfg.device));
-    CK(cudaMemcpyAsync(x->hio + 16, &x->b.sc->smax_last, 2 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    CK(cudaMemcpyAsync(x->hio + 16, &x->rec.sc->smax_last, 2 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
     int rc = sync_and_check(x);
     if (rc) return rc;
     if (smax) *smax = x->hio[16];
@@ -404,6 +438,36 @@ int imhd_wave_speeds(imhd_box* x, double* smax, double* delv_max) {
 }
 
 long long imhd_launch_count(imhd_box* x) { return x ? x->b.launches : 0; }
+
+int imhd_fourier_field(imhd_box* x, int target, const int* kvec, const double* amp, int nmodes, double scale) {
+    if (!x || nmodes < 0 || (nmodes > 0 && (!kvec || !amp))) return fail(IMHD_E_ARG, "bad argument");
+    if (target != 0 && target != 1) return fail(IMHD_E_ARG, "target must be 0 (velocity) or 1 (force)");
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    if (target == 1 && !x->rec.delv) {
+        if (cudaMalloc(&x->rec.delv, 3 * (size_t)x->rec.n * x->esz) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(IMHD_E_NOMEM, "device allocation of the force field failed");
+        }
+        if ((rc = upload_table(x))) return rc;
+    }
+    int* kd = nullptr;
+    double* ad = nullptr;
+    if (nmodes) {
+        CK(cudaMallocAsync((void**)&kd, (size_t)nmodes * 3 * sizeof(int), x->b.st));
+        CK(cudaMallocAsync((void**)&ad, (size_t)nmodes * 6 * sizeof(double), x->b.st));
+        CK(cudaMemcpyAsync(kd, kvec, (size_t)nmodes * 3 * sizeof(int), cudaMemcpyHostToDevice, x->b.st));
+        CK(cudaMemcpyAsync(ad, amp, (size_t)nmodes * 6 * sizeof(double), cudaMemcpyHostToDevice, x->b.st));
+    }
+    cudaError_t e = is64(x) ? imhd::run_ou_field<double>(x->b.st, x->rec, x->cur, target, kd, ad, nmodes, scale)
+                            : imhd::run_ou_field<float>(x->b.st, x->rec, x->cur, target, kd, ad, nmodes, scale);
+    x->b.launches += 1;
+    if (kd) cudaFreeAsync(kd, x->b.st);
+    if (ad) cudaFreeAsync(ad, x->b.st);
+    CK(e);
+    if (target == 1) x->have_force = true;
+    return sync_and_check(x);
+}
 
 int imhd_set_stream(imhd_box* x, void* stream) {
     if (!x) return fail(IMHD_E_ARG, "null argument");

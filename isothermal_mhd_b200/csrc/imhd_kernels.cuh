@@ -30,6 +30,46 @@
 
 namespace imhd {
 
+struct Dims {
+    int nx, ny, nz;
+    int n;        // nx*ny*nz (< 2^31)
+};
+
+// Box of the current block and the block's index within that box.  ONE: the
+// launch covers a single box whose record is a kernel parameter (read from
+// the constant bank, no dependent loads); otherwise the block looks its box up
+// in the device table.
+template <bool ONE>
+__device__ __forceinline__ BoxRec resolve(const BatchArgs& ba, int kind, int& local) {
+    if constexpr (ONE) {
+        local = (int)blockIdx.x;
+        return ba.one;
+    } else {
+        int b = __ldg(ba.blk2box[kind] + blockIdx.x);
+        local = (int)blockIdx.x - __ldg(ba.prefix + kind * (ba.nbox + 1) + b);
+        return ba.boxes[b];
+    }
+}
+// Box b of the table (the kernels that run one thread or block per box).
+__device__ __forceinline__ BoxRec box_at(const BatchArgs& ba, int b) { return ba.use_one ? ba.one : ba.boxes[b]; }
+__device__ __forceinline__ Dims dims_of(const BoxRec& r) { return Dims{r.nx, r.ny, r.nz, r.n}; }
+// kKindCell decomposition: ceil(nx/kBX) blocks per (j,k) row
+// (a single box launches a 3D grid (nbx, ny, nz) and needs no division)
+template <bool ONE>
+__device__ __forceinline__ void decode_cell(int local, const Dims& dm, int& i, int& j, int& k) {
+    if constexpr (ONE) {
+        i = (int)(blockIdx.x * kBX + threadIdx.x);
+        j = (int)blockIdx.y;
+        k = (int)blockIdx.z;
+    } else {
+        int nbx = (dm.nx + kBX - 1) / kBX;
+        int bx = local % nbx, rest = local / nbx;
+        j = rest % dm.ny;
+        k = rest / dm.ny;
+        i = bx * kBX + (int)threadIdx.x;
+    }
+}
+
 __device__ __forceinline__ int wrap_up(int i, int n) { return (i + 1 == n) ? 0 : i + 1; }
 __device__ __forceinline__ int wrap_dn(int i, int n) { return (i == 0) ? n - 1 : i - 1; }
 __device__ __forceinline__ int wrap_any(int i, int n) { i %= n; return i < 0 ? i + n : i; }
@@ -98,12 +138,20 @@ template <int D> struct Rot {
 // First-order interface fluxes (compute_{x,y,z}fluxes_3d with
 // corrector_stage = .FALSE., vanleer_mod.f90:441-478): left/right states are
 // the cell values, the normal field the face value.
-template <class T, int SOLVER, int D>
-__global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
-                                                   T asqr, unsigned long long* smax_slots) {
+template <class T, int SOLVER, int D, bool ONE>
+__global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
     using R = Rot<D>;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubCell), local);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[0];
+    T* __restrict__ F = (T*)rp.F;
+    const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
+    unsigned long long* smax_slots = sc->smax_slots;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     bool valid = i < dm.nx;
     T smax = T(0);
     if (valid) {
@@ -129,7 +177,7 @@ __global__ void __launch_bounds__(128) k_pred_flux(const T* __restrict__ S, T* _
         Fd[4 * (size_t)dm.n + c] = Fo[5];
         Fd[5 * (size_t)dm.n + c] = Fo[6];
     }
-    block_atomic_max<128>(smax_slots, (double)smax);
+    block_atomic_max<kBX>(smax_slots, (double)smax);
 }
 
 // ============================================================ corrector flux
@@ -164,12 +212,30 @@ __device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int 
 // marches along the sweep direction over a segment of faces, keeping the
 // primitive window w(a-1..a+2) and the slopes delw(a), delw(a+1) in
 // registers.  Loads stay coalesced along x.
-template <class T, int SOLVER, int D>
-__global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S, T* __restrict__ F, Dims dm,
-                                                         int seg, T cs, T asqr, unsigned long long* smax_slots) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int o = blockIdx.y;                         // k for D=1, j for D=2
-    int a0 = blockIdx.z * seg;
+template <class T, int SOLVER, int D, bool ONE>
+__global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, D == 1 ? kSubMarchY : kSubMarchZ), local);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[1];   // half-step state
+    T* __restrict__ F = (T*)rp.F;
+    const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
+    unsigned long long* smax_slots = sc->smax_slots;
+    const int seg = kSeg;
+    int bx, o, a0;                              // o: k for D=1, j for D=2
+    if constexpr (ONE) {                        // grid (nbx, nother, nseg)
+        bx = (int)blockIdx.x; o = (int)blockIdx.y; a0 = (int)blockIdx.z * seg;
+    } else {
+        int nbx = (dm.nx + kBX - 1) / kBX;
+        int nother = (D == 1) ? dm.nz : dm.ny;
+        int rest = local / nbx;
+        bx = local % nbx;
+        o = rest % nother;
+        a0 = (rest / nother) * seg;
+    }
+    int i = bx * kBX + (int)threadIdx.x;
     int na = (D == 1) ? dm.ny : dm.nz;
     int a1 = min(a0 + seg, na);
     bool valid = i < dm.nx;
@@ -200,19 +266,34 @@ __global__ void __launch_bounds__(128) k_corr_flux_march(const T* __restrict__ S
             bnA = bnB; bnB = bnC;
         }
     }
-    block_atomic_max<128>(smax_slots, (double)smax);
+    block_atomic_max<kBX>(smax_slots, (double)smax);
 }
 
 // Sweep along x: a block covers TX faces of one (j,k) row; primitives of the
 // TX+3 cells and the TX+1 slopes are staged in shared memory.
-template <class T, int SOLVER, int TX>
-__global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
-                                                    T asqr, unsigned long long* smax_slots) {
+template <class T, int SOLVER, int TX, bool ONE>
+__global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
     __shared__ T sw[6][TX + 3];
     __shared__ T sbn[TX + 3];
     __shared__ T sd[6][TX + 1];
-    int i0 = blockIdx.x * TX;
-    int j = blockIdx.y, k = blockIdx.z;
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubXTile), local);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[1];   // half-step state
+    T* __restrict__ F = (T*)rp.F;
+    const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
+    unsigned long long* smax_slots = sc->smax_slots;
+    int i0, j, k;
+    if constexpr (ONE) {                        // grid (nbt, ny, nz)
+        i0 = (int)blockIdx.x * TX; j = (int)blockIdx.y; k = (int)blockIdx.z;
+    } else {
+        int nbt = (dm.nx + TX - 1) / TX;
+        i0 = (local % nbt) * TX;
+        j = (local / nbt) % dm.ny;
+        k = (local / nbt) / dm.ny;
+    }
     int row = dm.nx * (j + dm.ny * k);
     for (int t = threadIdx.x; t < TX + 3; t += TX) {
         int ii = wrap_any(i0 - 1 + t, dm.nx);
@@ -246,7 +327,7 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* 
         riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
-    block_atomic_max<128>(smax_slots, (double)smax);
+    block_atomic_max<TX>(smax_slots, (double)smax);
 }
 
 // Sweep along x over whole rows: one block per (j,k) row.  The primitives,
@@ -254,15 +335,28 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(const T* __restrict__ S, T* 
 // wrap is an index wrap inside the row, so every cell's slope is computed
 // exactly once (the tiled kernel above recomputes one slope per tile and
 // stages a halo).  Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
-template <class T, int SOLVER>
-__global__ void __launch_bounds__(256) k_corr_flux_xrow(const T* __restrict__ S, T* __restrict__ F, Dims dm, T cs,
-                                                        T asqr, unsigned long long* smax_slots) {
+template <class T, int SOLVER, bool ONE>
+__global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
     extern __shared__ __align__(16) unsigned char xrow_smem[];
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubXRow), local);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[1];   // half-step state
+    T* __restrict__ F = (T*)rp.F;
+    const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
+    unsigned long long* smax_slots = sc->smax_slots;
     const int nx = dm.nx;
     T* sw = (T*)xrow_smem;     // [6][nx] primitives
     T* sbn = sw + 6 * nx;      // [nx] face field at i+1/2
     T* sd = sbn + nx;          // [6][nx] slopes
-    int j = blockIdx.x, k = blockIdx.y;
+    int j, k;
+    if constexpr (ONE) {                        // grid (ny, nz)
+        j = (int)blockIdx.x; k = (int)blockIdx.y;
+    } else {
+        j = local % dm.ny; k = local / dm.ny;
+    }
     int row = nx * (j + dm.ny * k);
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         T w[6], bn;
@@ -335,11 +429,18 @@ __device__ __forceinline__ void upwind_pair(T v, T L14, T R14, T L34, T R34, T& 
     else { o14 = T(0.5) * (L14 + R14); o34 = T(0.5) * (L34 + R34); }
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_corner_emf(const T* __restrict__ S, const T* __restrict__ F,
-                                                    T* __restrict__ E, Dims dm) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_corner_emf(BatchArgs ba, int half_step_state) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    Scalars* scb = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
+    const T* __restrict__ F = (const T*)rp.F;
+    T* __restrict__ E = (T*)rp.E;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     if (i >= dm.nx) return;
     const int n = dm.n;
     int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny), kp = wrap_up(k, dm.nz);
@@ -444,14 +545,25 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
     return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_update(const T* __restrict__ S0, const T* __restrict__ F,
-                                                const T* __restrict__ E, T* __restrict__ Sout, Dims dm,
-                                                const Scalars* __restrict__ sc, double dt_scale, double dx, T asqr,
-                                                int do_cfl, unsigned long long* cmax_slots,
-                                                unsigned long long* floor_hits, unsigned int* status) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_update(BatchArgs ba, double dt_scale, int final_stage) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ Sout = (T*)rp.S[1];
+    const T* __restrict__ F = (const T*)rp.F;
+    const T* __restrict__ E = (const T*)rp.E;
+    const double dx = rp.dx;
+    const T asqr = (T)(rp.cs * rp.cs);
+    const int do_cfl = final_stage && !sc->drive;
+    unsigned long long* cmax_slots = sc->cmax_slots;
+    unsigned long long* floor_hits = &sc->floor_hits;
+    unsigned int* status = &sc->status;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     bool valid = i < dm.nx;
     double cmax = 0.0;
     if (valid) {
@@ -499,7 +611,7 @@ __global__ void __launch_bounds__(128) k_update(const T* __restrict__ S0, const 
               isfinite(by) && isfinite(bz)))
             atomicOr(status, 2u);
     }
-    if (do_cfl) block_atomic_max<128>(cmax_slots, cmax);
+    if (do_cfl) block_atomic_max<kBX>(cmax_slots, cmax);
 }
 
 // ============================================================ passive scalars
@@ -518,11 +630,19 @@ __device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int c
 // Predictor: s_h = s - (dt/2dx) sum_d v_d (F_d(i+1/2) - F_d(i-1/2)) with
 // first-order upwind fluxes and the step-start velocity (passive_mod.f90:
 // 133-157, 204-224, 562-590).
-template <class T>
-__global__ void __launch_bounds__(128) k_passive_pred(const T* __restrict__ S0, T* __restrict__ SH, Dims dm,
-                                                      int npass, const Scalars* __restrict__ sc, double dx) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_passive_pred(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const Scalars* sc = rp.sc;
+    const int npass = rp.npass;
+    if (!rp.active || npass == 0) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ SH = (T*)rp.SH;
+    const double dx = rp.dx;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     if (i >= dm.nx) return;
     const int n = dm.n;
     T dtdx = (T)(0.5 * sc->dt / dx);
@@ -573,13 +693,23 @@ __device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict
     return T(0.5) * (vold + m1 * irho);
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_passive_corr(const T* __restrict__ S0, const T* __restrict__ SH,
-                                                      T* __restrict__ S1, Dims dm, int npass,
-                                                      const Scalars* __restrict__ sc, double dx, int drive,
-                                                      const T* __restrict__ mbnd, int plane_stride) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_passive_corr(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const Scalars* sc = rp.sc;
+    const int npass = rp.npass;
+    if (!rp.active || npass == 0) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ S1 = (T*)rp.S[1];
+    const T* __restrict__ SH = (const T*)rp.SH;
+    const double dx = rp.dx;
+    const int drive = sc->drive;
+    const T* __restrict__ mbnd = (const T*)rp.mbnd;
+    const int plane_stride = rp.plane_stride;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     if (i >= dm.nx) return;
     const int n = dm.n;
     T dtdx = (T)(sc->dt / dx);
@@ -635,12 +765,18 @@ __global__ void __launch_bounds__(128) k_passive_corr(const T* __restrict__ S0, 
 // ============================================================ forcing
 // get_rho_turb sums (turb_driver_mod.f90:158-186) over the step-start state,
 // per-block partial sums in FP64, reduced in a fixed order by k_force_reduce.
-template <class T>
-__global__ void __launch_bounds__(256) k_force_sums(const T* __restrict__ S0, const T* __restrict__ delv, Dims dm,
-                                                    double* __restrict__ partials) {
-    const int n = dm.n;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kRedThreads) k_force_sums(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindRed, local);
+    const Scalars* sc = rp.sc;
+    if (!rp.active || !sc->drive) return;
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    const T* __restrict__ delv = (const T*)rp.delv;
+    double* __restrict__ partials = rp.partials;
+    const int n = rp.n;
     double s[5] = {0, 0, 0, 0, 0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    for (int c = local * blockDim.x + threadIdx.x; c < n; c += rp.nred * blockDim.x) {
         double rho = (double)fld(S0, 0, n)[c];
         double d1 = (double)delv[c], d2 = (double)delv[(size_t)n + c], d3 = (double)delv[2 * (size_t)n + c];
         s[0] += rho * (d1 * d1 + d2 * d2 + d3 * d3);
@@ -660,16 +796,21 @@ __global__ void __launch_bounds__(256) k_force_sums(const T* __restrict__ S0, co
     if (threadIdx.x < 5) {
         double v = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
-        partials[(size_t)blockIdx.x * 5 + threadIdx.x] = v;
+        partials[(size_t)local * 5 + threadIdx.x] = v;
     }
 }
 
 // Sum the per-block partials in block order, then the normalisation of
 // add_random_force (turb_driver_mod.f90:411-434) for one rank.
-static __global__ void k_force_reduce(const double* __restrict__ partials, int nblocks, Scalars* sc, double dx, double edot,
-                               double dt_turb) {
+static __global__ void k_force_reduce(BatchArgs ba) {
+    const BoxRec rp = box_at(ba, blockIdx.x);   // one block of 32 threads per box
+    Scalars* sc = rp.sc;
+    if (!rp.active || !sc->drive) return;
+    const double* __restrict__ partials = rp.partials;
+    const int nblocks = rp.nred;
+    const double dx = rp.dx, edot = rp.edot, dt_turb = rp.dt_turb;
     __shared__ double acc[5][32];
-    int t = threadIdx.x;   // 32 threads
+    int t = threadIdx.x;
     for (int q = 0; q < 5; ++q) {
         double v = 0.0;
         for (int b = t; b < nblocks; b += 32) v += partials[(size_t)b * 5 + q];
@@ -704,12 +845,22 @@ static __global__ void k_force_reduce(const double* __restrict__ partials, int n
 // Kick m += constE (rho0 delv - <rho delv>) on the new state
 // (turb_driver_mod.f90:437-453), delv_max, the CFL maximum of the kicked
 // state, and the unforced boundary-plane momentum for k_passive_corr.
-template <class T>
-__global__ void __launch_bounds__(128) k_force_kick(const T* __restrict__ S0, T* __restrict__ S1,
-                                                    const T* __restrict__ delv, Dims dm, Scalars* sc, T asqr,
-                                                    T* __restrict__ mbnd, int plane_stride, int save_bnd) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_force_kick(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    Scalars* sc = rp.sc;
+    if (!rp.active || !sc->drive) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ S1 = (T*)rp.S[1];
+    const T* __restrict__ delv = (const T*)rp.delv;
+    T* __restrict__ mbnd = (T*)rp.mbnd;
+    const int plane_stride = rp.plane_stride;
+    const int save_bnd = rp.npass > 0;
+    const T asqr = (T)(rp.cs * rp.cs);
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     bool valid = i < dm.nx;
     double dvmax = 0.0, cmax = 0.0;
     if (valid) {
@@ -743,14 +894,21 @@ __global__ void __launch_bounds__(128) k_force_kick(const T* __restrict__ S0, T*
         cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
                                       fld(S1, 6, n)[c], asqr);
     }
-    block_atomic_max<128>(sc->dvmax_slots, dvmax);
-    block_atomic_max<128>(sc->cmax_slots, cmax);
+    block_atomic_max<kBX>(sc->dvmax_slots, dvmax);
+    block_atomic_max<kBX>(sc->cmax_slots, cmax);
 }
 
 // ============================================================ dt and maxima
 // compute_new_time_step (driver.f90:432-448) with the smax coupling of
 // get_max_speed_vanleer (vanleer_mod.f90:3323); resets the step maxima.
-static __global__ void k_finalize(Scalars* sc, double cour, double dx, int drive) {
+static __global__ void k_finalize(BatchArgs ba, int device_driven) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ba.nbox) return;
+    const BoxRec rp = box_at(ba, b);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const double cour = rp.cour, dx = rp.dx;
+    const int drive = sc->drive;
     double cell = 0.0, smax = 0.0, dvm = 0.0;
     for (int s = 0; s < kSlots; ++s) {
         cell = nmax(cell, __longlong_as_double((long long)sc->cmax_slots[s]));
@@ -768,13 +926,56 @@ static __global__ void k_finalize(Scalars* sc, double cour, double dx, int drive
     sc->smax_last = smax;
     sc->dvmax_last = dvm;
     sc->dt_next = c * dx / cmax;
+    sc->cur ^= 1;   // the new state is now current
+    if (!ba.use_one) {
+        BoxRec& tr = ba.boxes[b];
+        void* s0 = tr.S[0];
+        tr.S[0] = tr.S[1];
+        tr.S[1] = s0;
+    }
+    if (device_driven) {
+        // driver.f90:86-87 and :475 for this box
+        sc->t = sc->t + sc->dt;
+        sc->steps_done += 1;
+        if (sc->steps_done >= sc->steps_target || !(sc->t < sc->t_end) || (sc->status & 6u)) {
+            sc->active = 0;
+            if (!ba.use_one) ba.boxes[b].active = 0;
+        } else {
+            sc->dt = vmin(sc->t_end - sc->t, sc->dt_next);
+        }
+        sc->drive = 0;
+    }
+}
+
+// Drive decision of a device-driven step (driver.f90:57-70): a box drives
+// when t_turb falls in (t, t + dt]; then t_turb advances and dt halves.
+static __global__ void k_batch_begin(BatchArgs ba) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ba.nbox) return;
+    const BoxRec rp = box_at(ba, b);
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    int drive = 0;
+    if (sc->forcing && (sc->t_turb > sc->t) && (sc->t_turb <= sc->t + sc->dt)) {
+        drive = 1;
+        sc->t_turb = vmax(sc->t_turb + sc->dt_turb_sched, sc->t + 1.0e-2 * sc->dt);
+        sc->dt = 0.5 * sc->dt;
+    }
+    sc->drive = drive;
 }
 
 // cell fast-speed maximum of a state (imhd_max_speed)
-template <class T>
-__global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T asqr, unsigned long long* out_slots) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int j = blockIdx.y, k = blockIdx.z;
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_cfl(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    Scalars* sc = rp.sc;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[0];
+    const T asqr = (T)(rp.cs * rp.cs);
+    unsigned long long* out_slots = sc->cfl_slots;
+    int i, j, k;
+    decode_cell<ONE>(local, dm, i, j, k);
     double cm = 0.0;
     if (i < dm.nx) {
         const int n = dm.n;
@@ -782,17 +983,23 @@ __global__ void __launch_bounds__(128) k_cfl(const T* __restrict__ S, Dims dm, T
         cm = (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],
                                     fld(S, 4, n)[c], fld(S, 5, n)[c], fld(S, 6, n)[c], asqr);
     }
-    block_atomic_max<128>(out_slots, cm);
+    block_atomic_max<kBX>(out_slots, cm);
 }
 
 // ============================================================ diagnostics
 // compute_KE (driver.f90:518-553) and compute_divB (:492-515) as FP64
 // per-block partials; reduced by k_diag_reduce in block order.
-template <class T>
-__global__ void __launch_bounds__(256) k_diag(const T* __restrict__ S, Dims dm, double* __restrict__ partials) {
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kRedThreads) k_diag(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindRed, local);
+    const Scalars* sc = rp.sc;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)rp.S[0];
+    double* __restrict__ partials = rp.partials;
     const int n = dm.n;
     double s[6] = {0, 0, 0, 0, 0, 0};
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+    for (int c = local * blockDim.x + threadIdx.x; c < n; c += rp.nred * blockDim.x) {
         int i = c % dm.nx, j = (c / dm.nx) % dm.ny, k = c / (dm.nx * dm.ny);
         double rho = vmin(vmax((double)fld(S, 0, n)[c], 1.0e-15), 1.0e10);
         double mx = (double)fld(S, 1, n)[c], my = (double)fld(S, 2, n)[c], mz = (double)fld(S, 3, n)[c];
@@ -817,12 +1024,17 @@ __global__ void __launch_bounds__(256) k_diag(const T* __restrict__ S, Dims dm, 
     if (threadIdx.x < 6) {
         double v = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
-        partials[(size_t)blockIdx.x * 6 + threadIdx.x] = v;
+        partials[(size_t)local * 6 + threadIdx.x] = v;
     }
 }
 
-static __global__ void k_diag_reduce(const double* __restrict__ partials, int nblocks, Scalars* sc, double dx) {
+static __global__ void k_diag_reduce(BatchArgs ba) {
     if (threadIdx.x != 0) return;
+    const BoxRec rp = box_at(ba, blockIdx.x);   // one block per box
+    Scalars* sc = rp.sc;
+    const double* __restrict__ partials = rp.partials;
+    const int nblocks = rp.nred;
+    const double dx = rp.dx;
     double s[6] = {0, 0, 0, 0, 0, 0};
     for (int b = 0; b < nblocks; ++b)
         for (int q = 0; q < 6; ++q) s[q] += partials[(size_t)b * 6 + q];
@@ -833,6 +1045,40 @@ static __global__ void k_diag_reduce(const double* __restrict__ partials, int nb
     sc->diag[3] = s[3] * dx3;
     sc->diag[4] = s[4] * dx3;
     sc->diag[5] = s[5];
+}
+
+// ============================================================ Fourier fields
+// v_d(x) = sum_m 2 Re(A_{m,d} exp(2 pi i k_m . x)) on the cell centres
+// x = ((i+1/2)/nx, (j+1/2)/ny, (k+1/2)/nz): the solenoidal OU forcing and
+// initial velocity fields (shells 1 <= |k| <= 2 carry ~16 modes).  target 0
+// adds rho * scale * v to the momentum of state S[cur]; target 1 writes
+// scale * v to the force field.  Phases are reduced in FP64.
+template <class T>
+__global__ void __launch_bounds__(kBX) k_fourier_field(BoxRec r, int cur, int target, const int* __restrict__ kv,
+                                                       const double* __restrict__ amp, int nm, double scale) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= r.n) return;
+    int i = c % r.nx, j = (c / r.nx) % r.ny, k = c / (r.nx * r.ny);
+    double x = (i + 0.5) / r.nx, y = (j + 0.5) / r.ny, z = (k + 0.5) / r.nz;
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int m = 0; m < nm; ++m) {
+        double ph = kv[3 * m] * x + kv[3 * m + 1] * y + kv[3 * m + 2] * z;
+        ph = 2.0 * (ph - floor(ph));
+        double s, co;
+        sincospi(ph, &s, &co);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] += 2.0 * (amp[6 * m + 2 * d] * co - amp[6 * m + 2 * d + 1] * s);
+    }
+    if (target == 0) {
+        T* S = (T*)r.S[cur];
+        double rho = (double)S[c];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) S[(size_t)(1 + d) * r.n + c] = (T)((double)S[(size_t)(1 + d) * r.n + c] + rho * scale * v[d]);
+    } else {
+        T* D = (T*)r.delv;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) D[(size_t)d * r.n + c] = (T)(scale * v[d]);
+    }
 }
 
 // ============================================================ host transfer

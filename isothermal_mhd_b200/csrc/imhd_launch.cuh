@@ -1,7 +1,14 @@
-// imhd_launch.cuh -- host-side launch sequence of one step, templated on the
-// arithmetic type.  Included by imhd_f64.cu (compiled with --fmad=false for
-// bit parity with the FP64 oracle) and imhd_f32.cu (FMA on), each of which
-// instantiates one precision.
+// imhd_launch.cuh -- host-side launch sequence of one step over a table of
+// boxes (one box or a batch), templated on the arithmetic type.  Included by
+// imhd_f64.cu (compiled with --fmad=false for bit parity with the FP64
+// oracle) and imhd_f32.cu (FMA on), each of which instantiates one precision.
+//
+// Every launch covers all boxes of the table: the grid is the sum of the
+// boxes' blocks for that kernel's decomposition (BatchDev::totals).  A single
+// box travels in the kernel parameters (kernels instantiated with ONE); in a
+// batch each block reads its box from the block -> box table.  A step never
+// reads the host: dt, the drive flag and the current state buffer are device
+// scalars of each box, so the sequence can be captured in a CUDA graph.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -10,158 +17,204 @@
 
 namespace imhd {
 
-inline void mark(BoxDev& b, int stage) {
+inline void mark(BatchDev& b, int stage) {
     if (!b.prof) return;
     cudaEventRecord(b.ev[stage], b.st);
     b.prof_mask |= 1u << stage;
 }
 
-constexpr int kBX = 128;       // threads along x of the per-cell kernels
-constexpr int kTX = 128;       // faces per block of the x sweep
-constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
-constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
+// Grid of a launch of decomposition `kind`: the table's total block count, or
+// for a single box the 3D grid whose block indices the kernels read directly.
+template <bool ONE>
+static dim3 grid_of(const BatchDev& b, int kind) {
+    if constexpr (!ONE) {
+        return dim3((unsigned)b.totals[kind]);
+    } else {
+        const BoxRec& r = b.a.one;
+        unsigned nbx = (unsigned)((r.nx + kBX - 1) / kBX);
+        if (kind == kKindCell) return dim3(nbx, r.ny, r.nz);
+        if (kind == kKindRed) return dim3((unsigned)r.nred);
+        switch ((kind - kKindSolver0) % 5) {
+            case kSubCell: return dim3(nbx, r.ny, r.nz);
+            case kSubXRow: return dim3(r.ny, r.nz);
+            case kSubXTile: return dim3((unsigned)((r.nx + kTX - 1) / kTX), r.ny, r.nz);
+            case kSubMarchY: return dim3(nbx, r.nz, (unsigned)((r.ny + kSeg - 1) / kSeg));
+            default: return dim3(nbx, r.ny, (unsigned)((r.nz + kSeg - 1) / kSeg));
+        }
+    }
+}
 
-template <class T, int SOLVER>
-static void launch_fluxes_pred(BoxDev& b) {
-    const Dims& dm = b.dm;
-    dim3 blk(kBX), grd((dm.nx + kBX - 1) / kBX, dm.ny, dm.nz);
-    const T* S = (const T*)b.A;
-    T* F = (T*)b.F;
-    T cs = (T)b.cs, asqr = (T)(b.cs * b.cs);
-    mark(b, kStPredFlux);
-    k_pred_flux<T, SOLVER, 0><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
-    k_pred_flux<T, SOLVER, 1><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
-    k_pred_flux<T, SOLVER, 2><<<grd, blk, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+template <class T, int SOLVER, bool ONE>
+static void launch_fluxes_pred(BatchDev& b) {
+    if (b.totals[solver_kind(SOLVER, kSubCell)] == 0) return;
+    dim3 g = grid_of<ONE>(b, solver_kind(SOLVER, kSubCell));
+    k_pred_flux<T, SOLVER, 0, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    k_pred_flux<T, SOLVER, 1, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    k_pred_flux<T, SOLVER, 2, ONE><<<g, kBX, 0, b.st>>>(b.a);
     b.launches += 3;
 }
 
-template <class T, int SOLVER>
-static void launch_fluxes_corr(BoxDev& b) {
-    const Dims& dm = b.dm;
-    const T* S = (const T*)b.B;
-    T* F = (T*)b.F;
-    T cs = (T)b.cs, asqr = (T)(b.cs * b.cs);
-    mark(b, kStCorrFluxX);
-    size_t row_smem = 13 * (size_t)dm.nx * sizeof(T);
-    if (row_smem <= kRowSmemMax) {
-        static bool attr_set[64] = {};   // per instantiation and device
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-            cudaFuncSetAttribute(k_corr_flux_xrow<T, SOLVER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kRowSmemMax);
-            if (dev >= 0 && dev < 64) attr_set[dev] = true;
-        }
-        int bd = dm.nx >= 256 ? 256 : ((dm.nx + 31) / 32) * 32;
-        k_corr_flux_xrow<T, SOLVER><<<dim3(dm.ny, dm.nz), bd, row_smem, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
-    } else {
-        dim3 gx((dm.nx + kTX - 1) / kTX, dm.ny, dm.nz);
-        k_corr_flux_x<T, SOLVER, kTX><<<gx, kTX, 0, b.st>>>(S, F, dm, cs, asqr, b.sc->smax_slots);
+// The x-row sweep needs more than 48 KiB of dynamic shared memory for long
+// rows; the opt-in is per kernel and device and is done outside any capture.
+template <class T, int SOLVER, bool ONE>
+static void ensure_xrow_attr() {
+    static bool attr_set[64] = {};   // per instantiation and device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        cudaFuncSetAttribute(k_corr_flux_xrow<T, SOLVER, ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRowSmemMax);
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
-    dim3 gy((dm.nx + kBX - 1) / kBX, dm.nz, (dm.ny + kSeg - 1) / kSeg);
-    mark(b, kStCorrFluxY);
-    k_corr_flux_march<T, SOLVER, 1><<<gy, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, b.sc->smax_slots);
-    dim3 gz((dm.nx + kBX - 1) / kBX, dm.ny, (dm.nz + kSeg - 1) / kSeg);
-    mark(b, kStCorrFluxZ);
-    k_corr_flux_march<T, SOLVER, 2><<<gz, kBX, 0, b.st>>>(S, F, dm, kSeg, cs, asqr, b.sc->smax_slots);
-    b.launches += 3;
 }
 
 template <class T>
-cudaError_t run_step(BoxDev& b, int drive) {
-    const Dims& dm = b.dm;
-    dim3 blk(kBX), grd((dm.nx + kBX - 1) / kBX, dm.ny, dm.nz);
-    T asqr = (T)(b.cs * b.cs);
-    const T* A = (const T*)b.A;
-    T* Bs = (T*)b.B;
-    b.prof_mask = 0;
-    if (drive) {
-        mark(b, kStForceSums);
-        k_force_sums<T><<<b.nred, 256, 0, b.st>>>(A, (const T*)b.delv, dm, b.partials);
-        k_force_reduce<<<1, 32, 0, b.st>>>(b.partials, b.nred, b.sc, b.dx, b.edot, b.dt_turb);
-        b.launches += 2;
-    }
-    // predictor: first-order fluxes, EMFs, half-dt update into B
-    switch (b.riemann) {
-        case 1: launch_fluxes_pred<T, 1>(b); break;
-        case 2: launch_fluxes_pred<T, 2>(b); break;
-        default: launch_fluxes_pred<T, 3>(b); break;
-    }
-    mark(b, kStPredEmf);
-    k_corner_emf<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (T*)b.E, dm);
-    mark(b, kStPredUpdate);
-    k_update<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (const T*)b.E, Bs, dm, b.sc, 0.5, b.dx, asqr, 0,
-                                       b.sc->cmax_slots, &b.sc->floor_hits, &b.sc->status);
-    b.launches += 2;
-    // corrector: characteristic PLM fluxes of the half-step state, EMFs,
-    // full-dt update of the step-start state into B
-    switch (b.riemann) {
-        case 1: launch_fluxes_corr<T, 1>(b); break;
-        case 2: launch_fluxes_corr<T, 2>(b); break;
-        default: launch_fluxes_corr<T, 3>(b); break;
-    }
-    mark(b, kStCorrEmf);
-    k_corner_emf<T><<<grd, blk, 0, b.st>>>(Bs, (const T*)b.F, (T*)b.E, dm);
-    mark(b, kStFinalUpdate);
-    k_update<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.F, (const T*)b.E, Bs, dm, b.sc, 1.0, b.dx, asqr, drive ? 0 : 1,
-                                       b.sc->cmax_slots, &b.sc->floor_hits, &b.sc->status);
-    b.launches += 2;
-    if (drive) {
-        mark(b, kStForceKick);
-        k_force_kick<T><<<grd, blk, 0, b.st>>>(A, Bs, (const T*)b.delv, dm, b.sc, asqr, (T*)b.mbnd, b.plane_stride,
-                                               b.npass > 0 ? 1 : 0);
+cudaError_t prepare_launch(BatchDev& b) {
+    if (b.has_solver[1]) { ensure_xrow_attr<T, 1, true>(); ensure_xrow_attr<T, 1, false>(); }
+    if (b.has_solver[2]) { ensure_xrow_attr<T, 2, true>(); ensure_xrow_attr<T, 2, false>(); }
+    if (b.has_solver[3]) { ensure_xrow_attr<T, 3, true>(); ensure_xrow_attr<T, 3, false>(); }
+    return cudaGetLastError();
+}
+
+template <class T, int SOLVER, bool ONE>
+static void launch_fluxes_corr_x(BatchDev& b) {
+    if (b.totals[solver_kind(SOLVER, kSubXRow)]) {
+        dim3 gr = grid_of<ONE>(b, solver_kind(SOLVER, kSubXRow));
+        size_t smem = 13 * (size_t)b.row_nx_max * sizeof(T);
+        ensure_xrow_attr<T, SOLVER, ONE>();
+        int bd = b.row_nx_max >= 256 ? 256 : ((b.row_nx_max + 31) / 32) * 32;
+        k_corr_flux_xrow<T, SOLVER, ONE><<<gr, bd, smem, b.st>>>(b.a);
         b.launches += 1;
     }
-    if (b.npass > 0) {
+    if (b.totals[solver_kind(SOLVER, kSubXTile)]) {
+        dim3 gt = grid_of<ONE>(b, solver_kind(SOLVER, kSubXTile));
+        k_corr_flux_x<T, SOLVER, kTX, ONE><<<gt, kTX, 0, b.st>>>(b.a);
+        b.launches += 1;
+    }
+}
+
+template <class T, int SOLVER, int D, bool ONE>
+static void launch_fluxes_corr_march(BatchDev& b) {
+    const int kind = solver_kind(SOLVER, D == 1 ? kSubMarchY : kSubMarchZ);
+    if (b.totals[kind] == 0) return;
+    dim3 g = grid_of<ONE>(b, kind);
+    k_corr_flux_march<T, SOLVER, D, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    b.launches += 1;
+}
+
+template <class T, bool ONE>
+static cudaError_t run_step_t(BatchDev& b, int device_driven) {
+    const dim3 gc = grid_of<ONE>(b, kKindCell);
+    const int nfin = (b.a.nbox + 31) / 32;
+    b.prof_mask = 0;
+    if (device_driven) {
+        k_batch_begin<<<nfin, 32, 0, b.st>>>(b.a);
+        b.launches += 1;
+    }
+    if (b.drive_mode) {
+        mark(b, kStForceSums);
+        k_force_sums<T, ONE><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a);
+        k_force_reduce<<<b.a.nbox, 32, 0, b.st>>>(b.a);
+        b.launches += 2;
+    }
+    // predictor: first-order fluxes, EMFs, half-dt update into the other buffer
+    mark(b, kStPredFlux);
+    if (b.has_solver[1]) launch_fluxes_pred<T, 1, ONE>(b);
+    if (b.has_solver[2]) launch_fluxes_pred<T, 2, ONE>(b);
+    if (b.has_solver[3]) launch_fluxes_pred<T, 3, ONE>(b);
+    mark(b, kStPredEmf);
+    k_corner_emf<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 0);
+    mark(b, kStPredUpdate);
+    k_update<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 0.5, 0);
+    b.launches += 2;
+    // corrector: characteristic PLM fluxes of the half-step state, EMFs,
+    // full-dt update of the step-start state
+    mark(b, kStCorrFluxX);
+    if (b.has_solver[1]) launch_fluxes_corr_x<T, 1, ONE>(b);
+    if (b.has_solver[2]) launch_fluxes_corr_x<T, 2, ONE>(b);
+    if (b.has_solver[3]) launch_fluxes_corr_x<T, 3, ONE>(b);
+    mark(b, kStCorrFluxY);
+    if (b.has_solver[1]) launch_fluxes_corr_march<T, 1, 1, ONE>(b);
+    if (b.has_solver[2]) launch_fluxes_corr_march<T, 2, 1, ONE>(b);
+    if (b.has_solver[3]) launch_fluxes_corr_march<T, 3, 1, ONE>(b);
+    mark(b, kStCorrFluxZ);
+    if (b.has_solver[1]) launch_fluxes_corr_march<T, 1, 2, ONE>(b);
+    if (b.has_solver[2]) launch_fluxes_corr_march<T, 2, 2, ONE>(b);
+    if (b.has_solver[3]) launch_fluxes_corr_march<T, 3, 2, ONE>(b);
+    mark(b, kStCorrEmf);
+    k_corner_emf<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 1);
+    mark(b, kStFinalUpdate);
+    k_update<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 1.0, 1);
+    b.launches += 2;
+    if (b.drive_mode) {
+        mark(b, kStForceKick);
+        k_force_kick<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);
+        b.launches += 1;
+    }
+    if (b.any_pass) {
         mark(b, kStPassivePred);
-        k_passive_pred<T><<<grd, blk, 0, b.st>>>(A, (T*)b.SH, dm, b.npass, b.sc, b.dx);
+        k_passive_pred<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);
         mark(b, kStPassiveCorr);
-        k_passive_corr<T><<<grd, blk, 0, b.st>>>(A, (const T*)b.SH, Bs, dm, b.npass, b.sc, b.dx, drive,
-                                                 (const T*)b.mbnd, b.plane_stride);
+        k_passive_corr<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);
         b.launches += 2;
     }
     mark(b, kStFinalize);
-    k_finalize<<<1, 1, 0, b.st>>>(b.sc, b.cour, b.dx, drive);
+    k_finalize<<<nfin, 32, 0, b.st>>>(b.a, device_driven);
     b.launches += 1;
     if (b.prof) cudaEventRecord(b.ev[kStages], b.st);
     return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t run_max_speed(BoxDev& b) {
-    const Dims& dm = b.dm;
-    dim3 blk(kBX), grd((dm.nx + kBX - 1) / kBX, dm.ny, dm.nz);
-    cudaMemsetAsync(b.sc->cfl_slots, 0, sizeof(b.sc->cfl_slots), b.st);
-    k_cfl<T><<<grd, blk, 0, b.st>>>((const T*)b.A, dm, (T)(b.cs * b.cs), b.sc->cfl_slots);
+cudaError_t run_step(BatchDev& b, int device_driven) {
+    return b.a.use_one ? run_step_t<T, true>(b, device_driven) : run_step_t<T, false>(b, device_driven);
+}
+
+template <class T, bool ONE>
+static cudaError_t run_max_speed_t(BatchDev& b) {
+    k_cfl<T, ONE><<<grid_of<ONE>(b, kKindCell), kBX, 0, b.st>>>(b.a);
     b.launches += 1;
     return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t run_diag(BoxDev& b) {
-    k_diag<T><<<b.nred, 256, 0, b.st>>>((const T*)b.A, b.dm, b.partials);
-    k_diag_reduce<<<1, 32, 0, b.st>>>(b.partials, b.nred, b.sc, b.dx);
+cudaError_t run_max_speed(BatchDev& b) {
+    return b.a.use_one ? run_max_speed_t<T, true>(b) : run_max_speed_t<T, false>(b);
+}
+
+template <class T, bool ONE>
+static cudaError_t run_diag_t(BatchDev& b) {
+    k_diag<T, ONE><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a);
+    k_diag_reduce<<<b.a.nbox, 32, 0, b.st>>>(b.a);
     b.launches += 2;
     return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t run_from_f64(BoxDev& b, const double* src, void* dst) {
-    int n = b.dm.n;
+cudaError_t run_diag(BatchDev& b) {
+    return b.a.use_one ? run_diag_t<T, true>(b) : run_diag_t<T, false>(b);
+}
+
+template <class T>
+cudaError_t run_from_f64(cudaStream_t st, const double* src, void* dst, int n) {
     int blocks = (n + 255) / 256;
     if (blocks > 65535) blocks = 65535;
-    k_from_f64<T><<<blocks, 256, 0, b.st>>>(src, (T*)dst, n);
-    b.launches += 1;
+    k_from_f64<T><<<blocks, 256, 0, st>>>(src, (T*)dst, n);
     return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t run_to_f64(BoxDev& b, const void* src, double* dst) {
-    int n = b.dm.n;
+cudaError_t run_to_f64(cudaStream_t st, const void* src, double* dst, int n) {
     int blocks = (n + 255) / 256;
     if (blocks > 65535) blocks = 65535;
-    k_to_f64<T><<<blocks, 256, 0, b.st>>>((const T*)src, dst, n);
-    b.launches += 1;
+    k_to_f64<T><<<blocks, 256, 0, st>>>((const T*)src, dst, n);
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t run_ou_field(cudaStream_t st, const BoxRec& r, int cur, int target, const int* kv, const double* amp,
+                         int nm, double scale) {
+    int blocks = (r.n + kBX - 1) / kBX;
+    k_fourier_field<T><<<blocks, kBX, 0, st>>>(r, cur, target, kv, amp, nm, scale);
     return cudaGetLastError();
 }
 
@@ -169,9 +222,12 @@ cudaError_t run_to_f64(BoxDev& b, const void* src, double* dst) {
 
 #define IMHD_INSTANTIATE(T)                                                        \
     namespace imhd {                                                               \
-    template cudaError_t run_step<T>(BoxDev&, int);                                \
-    template cudaError_t run_max_speed<T>(BoxDev&);                                \
-    template cudaError_t run_diag<T>(BoxDev&);                                     \
-    template cudaError_t run_from_f64<T>(BoxDev&, const double*, void*);          \
-    template cudaError_t run_to_f64<T>(BoxDev&, const void*, double*);            \
+    template cudaError_t run_step<T>(BatchDev&, int);                              \
+    template cudaError_t prepare_launch<T>(BatchDev&);                             \
+    template cudaError_t run_max_speed<T>(BatchDev&);                              \
+    template cudaError_t run_diag<T>(BatchDev&);                                   \
+    template cudaError_t run_from_f64<T>(cudaStream_t, const double*, void*, int); \
+    template cudaError_t run_to_f64<T>(cudaStream_t, const void*, double*, int);   \
+    template cudaError_t run_ou_field<T>(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int, \
+                                         double);                                  \
     }

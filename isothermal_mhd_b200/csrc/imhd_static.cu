@@ -13,7 +13,7 @@
 // Limits and sharing:
 //  * the scratch array holds kStaticScratchBytes (48 MiB) on every GPU that
 //    loads the library, until the process exits; a box needs
-//    (21 + npass) * nx*ny*nz * (4 or 8) bytes plus 4 KiB, i.e. up to 64^3 in
+//    (21 + npass) * nx*ny*nz * (4 or 8) bytes plus 56 KiB, i.e. up to 64^3 in
 //    FP64 or about 80^3 in FP32 with two passive scalars.  Larger boxes are
 //    rejected with IMHD_E_ARG; use imhd_create / imhd_step for them;
 //  * every call on a device uses the same array and leaves its contents
@@ -28,12 +28,14 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/imhd.h"
+#include "imhd_table.h"
 #include "imhd_types.cuh"
 
 namespace imhd {
-template <class T> cudaError_t run_step(BoxDev&, int);
+template <class T> cudaError_t run_step(BatchDev&, int);
 const char* set_last_error(int code, const char* msg);
 }  // namespace imhd
 
@@ -41,6 +43,8 @@ namespace {
 
 constexpr size_t kStaticScratchBytes = size_t(48) << 20;   // 48 MiB
 constexpr size_t kScalarsBytes = 4096;                     // imhd::Scalars, rounded up
+constexpr size_t kTableBytes = 4096;                       // box record + block prefixes
+constexpr size_t kPartialBytes = 1024 * 6 * 8;             // reduction partials (unused: no forcing)
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_step_scratch[kStaticScratchBytes];
@@ -65,7 +69,7 @@ int scratch_address(int dev, unsigned char** out, std::string& err) {
     return IMHD_OK;
 }
 
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+using imhd::align256;
 
 }  // namespace
 
@@ -73,6 +77,8 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
                                 double cour, const void* state_in, void* state_out, double dt, double* dt_next,
                                 void* stream) {
     static_assert(sizeof(imhd::Scalars) <= kScalarsBytes, "scalar block outgrew its scratch slot");
+    static_assert(256 + sizeof(int) * imhd::kKinds * 2 <= kTableBytes && sizeof(imhd::BoxRec) <= 256,
+                  "box table outgrew its scratch slot");
     auto fail = [](int code, const std::string& m) { imhd::set_last_error(code, m.c_str()); return code; };
     if (precision != 32 && precision != 64) return fail(IMHD_E_ARG, "precision must be 32 or 64");
     if (nx < 4 || ny < 4 || nz < 4) return fail(IMHD_E_ARG, "every edge needs at least 4 cells");
@@ -83,7 +89,7 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     size_t esz = precision == 64 ? 8 : 4;
     size_t n = (size_t)nx * ny * nz;
     size_t fields_bytes = align256(18 * n * esz) + align256(3 * n * esz) + align256((size_t)npass * n * esz);
-    size_t need = kScalarsBytes + fields_bytes;
+    size_t need = kScalarsBytes + kTableBytes + kPartialBytes + fields_bytes;
     if (need > kStaticScratchBytes)
         return fail(IMHD_E_ARG, "box needs " + std::to_string(need) + " bytes of step scratch but imhd_step_static holds " +
                                     std::to_string(kStaticScratchBytes) +
@@ -98,31 +104,45 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     int rc = scratch_address(dev, &base, err);
     if (rc) return fail(rc, err);
 
-    imhd::BoxDev b;
-    b.dm.nx = nx; b.dm.ny = ny; b.dm.nz = nz; b.dm.n = (int)n;
-    b.riemann = riemann;
-    b.npass = npass;
-    b.cs = sound_speed;
-    int nmax = nx > ny ? nx : ny;
-    nmax = nmax > nz ? nmax : nz;
-    b.dx = 1.0 / (double)nmax;
-    b.cour = cour;
-    b.A = const_cast<void*>(state_in);
-    b.B = state_out;
-    b.sc = (imhd::Scalars*)base;
-    unsigned char* p = base + kScalarsBytes;
-    b.F = p;  p += align256(18 * n * esz);
-    b.E = p;  p += align256(3 * n * esz);
-    b.SH = npass ? (void*)p : nullptr;
+    imhd::BoxRec rec;
+    imhd::init_rec(rec, nx, ny, nz, npass, riemann, sound_speed, cour, 0.0, 0.0);
+    rec.S[0] = const_cast<void*>(state_in);
+    rec.S[1] = state_out;
+    unsigned char* p = base;
+    rec.sc = (imhd::Scalars*)p;  p += kScalarsBytes;
+    unsigned char* table = p;    p += kTableBytes;
+    rec.partials = (double*)p;   p += kPartialBytes;
+    rec.F = p;  p += align256(18 * n * esz);
+    rec.E = p;  p += align256(3 * n * esz);
+    rec.SH = npass ? (void*)p : nullptr;
+    rec.delv = nullptr;
+    rec.mbnd = nullptr;
+    imhd::BatchDev b;
+    b.precision = precision;
     b.st = (cudaStream_t)stream;
+    std::vector<imhd::BoxRec> recs(1, rec);
+    std::vector<int> prefix;
+    if (!imhd::build_prefix(recs, esz, prefix, b)) return fail(IMHD_E_ARG, "box too large for one launch");
+    b.a.boxes = (imhd::BoxRec*)table;
+    b.a.prefix = (const int*)(table + 256);
+    b.a.use_one = 1;                                      // the box travels in the launch parameters
+    b.a.one = rec;
+    b.drive_mode = 0;
+    imhd::Scalars init;
+    std::memset(&init, 0, sizeof(init));
+    init.active = 1;                                      // cur = 0: state_in is current
+    init.dt = dt;
 
     double host_io[2] = {dt, 0.0};
     unsigned status = 0;
-    e = cudaMemsetAsync(b.sc, 0, sizeof(imhd::Scalars), b.st);                       // slots start at zero
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&b.sc->dt, &host_io[0], sizeof(double), cudaMemcpyHostToDevice, b.st);
+    // the scalars (maxima slots included) start from zero on every call
+    e = cudaMemcpyAsync(rec.sc, &init, sizeof(init), cudaMemcpyHostToDevice, b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(table, &rec, sizeof(rec), cudaMemcpyHostToDevice, b.st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(table + 256, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice, b.st);
     if (e == cudaSuccess) e = precision == 64 ? imhd::run_step<double>(b, 0) : imhd::run_step<float>(b, 0);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&host_io[1], &b.sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, b.st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &b.sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&host_io[1], &rec.sc->dt_next, sizeof(double), cudaMemcpyDeviceToHost, b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &rec.sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, b.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b.st);
     if (e != cudaSuccess) return fail(IMHD_E_CUDA, std::string("imhd_step_static: ") + cudaGetErrorString(e));
     if (status & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");

@@ -1,0 +1,136 @@
+// imhd_table.h -- host side of a box table: per-box block counts of every
+// kernel decomposition, their prefixes, and the upload of the table.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <vector>
+
+#include "imhd_types.cuh"
+
+namespace imhd {
+
+inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+
+inline bool row_capable(int nx, size_t esz) { return 13 * (size_t)nx * esz <= kRowSmemMax; }
+
+inline int reduction_blocks(int n) {
+    int b = ceil_div(n, kRedThreads);
+    return b < kRedBlocksMax ? b : kRedBlocksMax;
+}
+
+// Blocks of box r for decomposition `kind`.
+inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
+    long nbx = ceil_div(r.nx, kBX);
+    if (kind == kKindCell) return nbx * r.ny * r.nz;
+    if (kind == kKindRed) return r.nred;
+    int solver = 1 + (kind - kKindSolver0) / 5;
+    int sub = (kind - kKindSolver0) % 5;
+    if (r.riemann != solver) return 0;
+    bool row = row_capable(r.nx, esz);
+    switch (sub) {
+        case kSubCell: return nbx * r.ny * r.nz;
+        case kSubXRow: return row ? (long)r.ny * r.nz : 0;
+        case kSubXTile: return row ? 0 : (long)ceil_div(r.nx, kTX) * r.ny * r.nz;
+        case kSubMarchY: return nbx * r.nz * ceil_div(r.ny, kSeg);
+        default: return nbx * r.ny * ceil_div(r.nz, kSeg);
+    }
+}
+
+// Prefix sums of every kind (kKinds rows of nbox+1 ints) and the launch
+// parameters of the table.  Returns false when a launch would exceed the
+// 2^31-1 block limit of a grid.
+inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vector<int>& prefix, BatchDev& bd);
+
+// Box of every block, per kind (for tables of more than one box).
+inline void build_blk2box(const std::vector<int>& prefix, int nbox, const BatchDev& bd,
+                          std::vector<std::vector<int>>& out) {
+    out.assign(kKinds, std::vector<int>());
+    for (int k = 0; k < kKinds; ++k) {
+        out[k].resize((size_t)bd.totals[k]);
+        for (int b = 0; b < nbox; ++b) {
+            int lo = prefix[(size_t)k * (nbox + 1) + b], hi = prefix[(size_t)k * (nbox + 1) + b + 1];
+            for (int i = lo; i < hi; ++i) out[k][(size_t)i] = b;
+        }
+    }
+}
+
+inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vector<int>& prefix, BatchDev& bd) {
+    int nbox = (int)recs.size();
+    prefix.assign((size_t)kKinds * (nbox + 1), 0);
+    for (int k = 0; k < kKinds; ++k) {
+        long acc = 0;
+        for (int b = 0; b < nbox; ++b) {
+            prefix[(size_t)k * (nbox + 1) + b] = (int)acc;
+            acc += blocks_of(recs[b], k, esz);
+            if (acc > 2147483647L) return false;
+        }
+        prefix[(size_t)k * (nbox + 1) + nbox] = (int)acc;
+        bd.totals[k] = (int)acc;
+    }
+    bd.row_nx_max = 0;
+    for (int s = 0; s < 4; ++s) bd.has_solver[s] = false;
+    bd.any_pass = false;
+    for (const BoxRec& r : recs) {
+        if (r.riemann >= 1 && r.riemann <= 3) bd.has_solver[r.riemann] = true;
+        if (r.npass > 0) bd.any_pass = true;
+        if (row_capable(r.nx, esz) && r.nx > bd.row_nx_max) bd.row_nx_max = r.nx;
+    }
+    bd.a.nbox = nbox;
+    return true;
+}
+
+// Fill the geometry fields of a box record from its configuration.
+inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, double cs, double cour, double edot,
+                     double dt_turb) {
+    std::memset(&r, 0, sizeof(r));
+    r.nx = nx; r.ny = ny; r.nz = nz; r.n = nx * ny * nz;
+    r.npass = npass;
+    r.riemann = riemann;
+    int pmax = ny * nz;
+    if (nx * nz > pmax) pmax = nx * nz;
+    if (nx * ny > pmax) pmax = nx * ny;
+    r.plane_stride = pmax;
+    r.nred = reduction_blocks(r.n);
+    int nmax = nx > ny ? nx : ny;
+    nmax = nmax > nz ? nmax : nz;
+    r.dx = 1.0 / (double)nmax;                 // vanleer_mod.f90:177, driver.f90:254
+    r.cs = cs;
+    r.cour = cour;
+    r.edot = edot;
+    r.dt_turb = dt_turb;
+    r.active = 1;
+}
+
+// Device bytes of one box's buffers (state x2, fluxes, EMFs, half-step
+// scalars, boundary planes, partial sums, scalars), each 256-byte aligned.
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+inline size_t box_bytes(const BoxRec& r, size_t esz, bool with_force) {
+    size_t n = (size_t)r.n, nf = 10 + (size_t)r.npass;
+    size_t b = 2 * align256(nf * n * esz) + align256(18 * n * esz) + align256(3 * n * esz);
+    if (r.npass) b += align256((size_t)r.npass * n * esz) + align256(6 * (size_t)r.plane_stride * esz);
+    if (with_force) b += align256(3 * n * esz);
+    b += align256((size_t)r.nred * 6 * 8) + align256(sizeof(Scalars));
+    return b;
+}
+// Carve the buffers of one box out of `base` (box_bytes of space).
+inline void carve_box(BoxRec& r, unsigned char* base, size_t esz, bool with_force) {
+    size_t n = (size_t)r.n, nf = 10 + (size_t)r.npass;
+    unsigned char* p = base;
+    r.S[0] = p; p += align256(nf * n * esz);
+    r.S[1] = p; p += align256(nf * n * esz);
+    r.F = p; p += align256(18 * n * esz);
+    r.E = p; p += align256(3 * n * esz);
+    if (r.npass) {
+        r.SH = p; p += align256((size_t)r.npass * n * esz);
+        r.mbnd = p; p += align256(6 * (size_t)r.plane_stride * esz);
+    } else {
+        r.SH = nullptr; r.mbnd = nullptr;
+    }
+    if (with_force) { r.delv = p; p += align256(3 * n * esz); } else r.delv = nullptr;
+    r.partials = (double*)p; p += align256((size_t)r.nred * 6 * 8);
+    r.sc = (Scalars*)p;
+}
+
+}  // namespace imhd

@@ -1,6 +1,6 @@
 // imhd_types.cuh -- plain data shared by the kernels, the launchers and the
-// C ABI: box dimensions, the device scalar block and the device-side view of
-// one box.
+// C ABI: the device scalar block of a box, the device record of a box and the
+// table that lets one launch cover many boxes.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -9,6 +9,13 @@
 namespace imhd {
 
 constexpr int kMaxPass = 8;
+constexpr int kSlots = 64;     // spread of the max reductions over addresses
+constexpr int kBX = 128;       // threads along x of the per-cell kernels
+constexpr int kTX = 128;       // faces per block of the tiled x sweep
+constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
+constexpr int kRedThreads = 256;
+constexpr int kRedBlocksMax = 1024;
+constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
 
 // stages of one step, in launch order (profiling slots)
 enum Stage {
@@ -16,17 +23,23 @@ enum Stage {
     kStCorrEmf, kStFinalUpdate, kStForceKick, kStPassivePred, kStPassiveCorr, kStFinalize, kStages
 };
 
-struct Dims {
-    int nx, ny, nz;
-    int n;        // nx*ny*nz (< 2^31)
+// Block-decomposition kinds: every launch covers the blocks of all boxes of a
+// table, laid end to end; prefix[kind][b] is the first block of box b.
+enum Kind {
+    kKindCell = 0,     // ceil(nx/kBX) * ny * nz blocks of kBX threads, one cell per thread
+    kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
+    kKindSolver0 = 2,  // + 5*(solver-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another solver
+    kKinds = 17
 };
+__host__ __device__ constexpr int solver_kind(int solver, int sub) { return kKindSolver0 + 5 * (solver - 1) + sub; }
+enum SolverSub { kSubCell = 0, kSubXRow = 1, kSubXTile = 2, kSubMarchY = 3, kSubMarchZ = 4 };
 
 // Device scalars of one box (FP64; maxima kept as the bit pattern of a
 // non-negative double so that atomicMax on the integer is a max on the value).
-constexpr int kSlots = 64;   // spread of the max reductions over addresses
-
 struct Scalars {
     double dt;                       // current dt (input of every step kernel)
+    int drive;                       // this step is a forcing step
+    int cur;                         // which state buffer holds the current state
     double dt_next;                  // COUR*dx/cmax of the last step
     double sums[5];                  // quad_term1, quad_term2, momx/y/z_avg
     double constE;
@@ -42,27 +55,54 @@ struct Scalars {
     unsigned long long cmax_slots[kSlots];
     unsigned long long dvmax_slots[kSlots];
     unsigned long long cfl_slots[kSlots];
+    // batched driver state (driver.f90:35-186 per box)
+    double t, t_end, t_turb, dt_turb_sched;
+    long long steps_done, steps_target;
+    int active, forcing;
 };
 
-struct BoxDev {
-    Dims dm;
-    int riemann = 1, npass = 0;
-    double cs = 1.0, dx = 1.0, cour = 0.35, edot = 1e-3, dt_turb = 0.05;
-    void* A = nullptr;      // current state (10 + npass fields)
-    void* B = nullptr;      // half-step, then new state
-    void* F = nullptr;      // 18 flux fields
-    void* E = nullptr;      // 3 corner EMF fields
-    void* SH = nullptr;     // npass half-step scalars
-    void* delv = nullptr;   // 3 forcing fields
-    void* mbnd = nullptr;   // 6 boundary planes of unforced momentum
-    int plane_stride = 0;
-    double* partials = nullptr;
-    int nred = 0;           // blocks of the reduction kernels
-    Scalars* sc = nullptr;
+// One box as the kernels see it.  S[0] is the current state (10 + npass
+// fields of n elements), S[1] the half-step / new state; a step ends by
+// swapping them (Scalars::cur counts the swaps for the host).
+struct BoxRec {
+    int nx, ny, nz, n;
+    int npass, riemann, plane_stride, nred;
+    int active, pad_;
+    double dx, cs, cour, edot, dt_turb;
+    void* S[2];
+    void* F;        // 18 flux fields
+    void* E;        // 3 corner EMF fields
+    void* SH;       // npass half-step scalars
+    void* delv;     // 3 forcing fields
+    void* mbnd;     // 6 boundary planes of unforced momentum
+    double* partials;   // nred * 6 FP64 partial sums
+    Scalars* sc;
+};
+
+// A table of boxes for one set of launches.  A single box travels by value
+// in the kernel parameters (use_one); a batch is a device table with, per
+// decomposition kind, the box of every block (blk2box) and the first block of
+// every box (prefix).
+struct BatchArgs {
+    BoxRec* boxes;
+    const int* prefix;               // [kKinds][nbox + 1]
+    const int* blk2box[kKinds];
+    int nbox;
+    int use_one;
+    BoxRec one;
+};
+
+// Host-side view of a table, owned by a single box or by a batch.
+struct BatchDev {
+    BatchArgs a;               // device pointers
+    int totals[kKinds];        // blocks per kind (grid sizes)
+    int row_nx_max = 0;        // largest nx among boxes using the x-row sweep
+    bool has_solver[4] = {false, false, false, false};
+    bool any_pass = false;
+    int drive_mode = 0;        // 0: no forcing, 1: every box drives (host decided), 2: per-box device flags
+    int precision = 64;
     cudaStream_t st = nullptr;
     long long launches = 0;
-    // optional per-stage timing: an event is recorded on `st` at the start of
-    // every stage that runs (prof_mask bit set) and once at the end
     bool prof = false;
     cudaEvent_t ev[kStages + 1] = {};
     unsigned prof_mask = 0;

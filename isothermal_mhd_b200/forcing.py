@@ -69,6 +69,18 @@ class OUForcing:
         f = np.exp(-float(dt) / self.tcorr)
         self.amp = f * self.amp + np.sqrt(max(0.0, 1.0 - f * f)) * self._draw()
 
+    def device_modes(self, rms=1.0):
+        """(kvec int32 (m,3), amp float64 (m,6), scale) for imhd_fourier_field:
+        the same field as :meth:`field` on the device.  The cell-centre phase is
+        applied there; the rms of |v| over the grid is 2 sum_m |a_m|^2 exactly
+        for wave numbers below the Nyquist limit, so the scale is analytic."""
+        kv = self.modes.astype(np.int32)
+        amp = np.empty((len(kv), 6))
+        amp[:, 0::2] = self.amp.real
+        amp[:, 1::2] = self.amp.imag
+        power = 2.0 * float(np.sum(np.abs(self.amp) ** 2))
+        return kv, amp, (rms / np.sqrt(power) if power > 0 else 0.0)
+
     def field(self, rms=1.0):
         """Real field v(x) = sum_k 2 Re(a_k exp(2 pi i k.x)) on the cell centres,
         shape (3, nz, ny, nx), scaled to the given rms of |v|."""
@@ -80,8 +92,8 @@ class OUForcing:
             for (kx, ky, kz), a in zip(self.modes, self.amp[:, c]):
                 # cell centres sit at (i+1/2) dx: fold the half-cell phase into a
                 ph = np.exp(1j * np.pi * (kx / nx + ky / ny + kz / nz) * (max(nx, ny, nz) * L))
-                if kx > 0:
-                    spec[kz % nz, ky % ny, kx] += 2.0 * a * ph
+                if kx > 0:      # irfftn adds the conjugate (-k) half itself
+                    spec[kz % nz, ky % ny, kx] += a * ph
                 else:   # kx == 0: Hermitian pair in the kx = 0 plane
                     spec[kz % nz, ky % ny, 0] += a * ph
                     spec[(-kz) % nz, (-ky) % ny, 0] += np.conj(a * ph)

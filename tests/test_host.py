@@ -43,6 +43,24 @@ def test_ou_field_is_solenoidal_and_normalised():
     assert P[(kk > 2.01) | (kk < 0.99)].sum() < 1e-20 * P.sum() + 1e-30
 
 
+def test_ou_field_equals_direct_mode_sum():
+    # v(x) = sum_m 2 Re(a_m exp(2 pi i k_m.x)) at the cell centres of a
+    # non-cubic box, and the analytic scale of device_modes gives its rms
+    n = (10, 8, 6)
+    f = forcing.OUForcing(n, seed=4)
+    v = f.field(rms=1.5)
+    kv, amp, scale = f.device_modes(rms=1.5)
+    nx, ny, nz = n
+    z, y, x = np.meshgrid((np.arange(nz) + 0.5) / nz, (np.arange(ny) + 0.5) / ny, (np.arange(nx) + 0.5) / nx,
+                          indexing="ij")
+    d = np.zeros((3, nz, ny, nx))
+    for (kx, ky, kz), a in zip(kv, amp):
+        ph = 2 * np.pi * (kx * x + ky * y + kz * z)
+        for c in range(3):
+            d[c] += 2.0 * (a[2 * c] * np.cos(ph) - a[2 * c + 1] * np.sin(ph))
+    np.testing.assert_allclose(v, scale * d, rtol=0, atol=1e-12)
+
+
 def test_ou_process_decorrelates_with_tcorr():
     f = forcing.OUForcing(16, tcorr=0.5, seed=3)
     a0 = f.amp.copy()
