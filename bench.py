@@ -56,6 +56,15 @@ def parse():
     ap.add_argument("--ref-n", type=int, default=128, help="edge of the CPU sample box")
     ap.add_argument("--ref-steps", type=int, default=None)
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--batched", type=int, default=512,
+                    help="boxes of the mixed-size batch measured beside the main line (0: skip)")
+    ap.add_argument("--batched-steps", type=int, default=50)
+    ap.add_argument("--served", type=int, default=400,
+                    help="requests of the Poisson stream through the serving loop (0: skip)")
+    ap.add_argument("--rate", type=float, default=200.0, help="mean arrival rate of the stream, requests/s")
+    ap.add_argument("--hbm-budget", type=float, default=150e9)
+    ap.add_argument("--loop-sample", type=int, default=128,
+                    help="boxes of the per-box loop arms, the first of the batch (0: all)")
     return ap.parse_args()
 
 
@@ -282,11 +291,21 @@ def run_ours(a, ws, rank, local):
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": sb[dom] * cells, "ms_per_launch": dom_ms}
 
+    batched = served = None
+    if a.batched > 0 or a.served > 0:
+        box.close()
+        box = None
+    if a.batched > 0:
+        batched = run_batched(a, local, stream, dist, dev)
+    if a.served > 0:
+        served = run_served(a, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         cpu = cpu_reference_sample(a, n_sample=a.ref_n, steps=a.ref_steps or 3, warmup=1)
 
-    box.close()
+    if box is not None:
+        box.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -306,8 +325,215 @@ def run_ours(a, ws, rank, local):
         "e2e": e2e,
         "cpu_baseline": cpu,
         "clocks": clk,
+        "batched": batched,
+        "served": served,
     }
     return line
+
+
+# ----------------------------------------------------------------- mixed-size batch
+def _build_box(obj, spec, i=None):
+    kv, av, sv, af, sf = spec.fields()
+    args = (i,) if i is not None else ()
+    obj.init_uniform(*args, rho=1.0, b0=spec.b0)
+    obj.fourier_field(*args, "velocity", kv, av, sv)
+    obj.fourier_field(*args, "force", kv, af, sf)
+
+
+def run_batched(a, local, stream, dist, dev):
+    """Mixed-size batch (512 boxes, edges U{32,48,64,96,128}, |B0| U[0.1,2],
+    Mach U[0.5,5], FP32 Roe + CT, 50 steps each, forcing on) through
+    imhd_batch_run, against the plain per-box loop of imhd_step calls with
+    the host driver loop.  Returns boxes/s and cell-updates/s of both arms."""
+    import torch
+    from isothermal_mhd_b200 import Batch, Box, ImhdError, driver, workloads
+    from isothermal_mhd_b200.batch import make_config
+
+    specs = workloads.batched_boxes(a.batched, steps=a.batched_steps, seed=a.seed)
+    cfgs = [make_config(s.n, precision=32, riemann=s.riemann, npass=s.npass, cour=a.cour, edot=s.edot,
+                        dt_turb=s.dt_turb, device=local) for s in specs]
+    cells_steps = sum(s.cells * s.steps for s in specs)
+    out = {"workload": "%d boxes, edges U{32,48,64,96,128}, |B0| U[0.1,2] random direction, rms Mach U[0.5,5], "
+                       "edot = Mach^3, FP32 Roe + PLM-char + CT, %d steps each, forcing on" % (len(specs),
+                                                                                           a.batched_steps),
+           "boxes": len(specs), "cells": sum(s.cells for s in specs)}
+    bt = Batch(cfgs)
+    bt.set_stream(stream.cuda_stream)
+
+    def setup():
+        for i, s in enumerate(specs):
+            _build_box(bt, s, i)
+            bt.schedule(i, s.steps, forcing=True)
+
+    setup()
+    bt.run(1)               # captures the step graph
+    setup()
+    launches0 = bt.launch_count
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    bt.run(a.batched_steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = [bt.clock(i) for i in range(len(specs))]
+    failed = [i for i, c in enumerate(clocks) if c["failed"]]
+    sample = [i for i in range(len(specs)) if i not in failed][:4]
+    batch_states = {i: bt.download(i) for i in sample}
+    done = sum(1 for c in clocks if not c["active"] and not c["failed"])
+    out["batch"] = {"ms": ms, "boxes_per_s": len(specs) / (ms / 1e3), "cell_updates_per_s": cells_steps / (ms / 1e3),
+                    "boxes_completed": done, "boxes_failed": len(failed),
+                    "graph_replays": a.batched_steps,
+                    "gpu_launches": bt.launch_count - launches0}
+    bt.close()
+    del bt
+
+    # plain per-box loops: one Box at a time, the host driver loop over
+    # imhd_step; FP64 is the plain method, FP32 the same loop at the batch's
+    # precision.  Both run the first `loop_sample` boxes (a random sample).
+    nloop = min(a.loop_sample or len(specs), len(specs))
+    sample_cells_steps = sum(s.cells * s.steps for s in specs[:nloop])
+    for prec in (64, 32):
+        loop_ms = 0.0
+        l1 = {}
+        nfail = 0
+        for i, s in enumerate(specs[:nloop]):
+            box = Box(s.n, precision=prec, riemann=s.riemann, npass=s.npass, cour=a.cour, edot=s.edot,
+                      dt_turb=s.dt_turb, device=local)
+            box.set_stream(stream.cuda_stream)
+            _build_box(box, s)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            try:
+                driver.run(box, t_end=1e30, maxsteps=s.steps + 1, forcing="device", dt_turb=s.dt_turb,
+                           record_dt=False)
+            except ImhdError:
+                nfail += 1          # NaN / zero speed: the box stops, as in the batch
+            torch.cuda.synchronize()
+            loop_ms += (time.perf_counter() - t0) * 1e3
+            if i in batch_states:
+                qa, ba, _ = box.download()
+                qb, bb, _ = batch_states[i]
+                # relative L1 per field of the FP32 batch against this loop
+                for f, (u, v) in enumerate([(qb[k], qa[k]) for k in range(7)] + [(bb[k], ba[k]) for k in range(3)]):
+                    den = float(np.sum(np.abs(v)))
+                    err = float(np.sum(np.abs(u - v)) / den) if den > 0 else float(np.sum(np.abs(u - v)))
+                    l1[f] = max(l1.get(f, 0.0), err)
+            box.close()
+        names = ["rho", "mx", "my", "mz", "bx_cc", "by_cc", "bz_cc", "bx_face", "by_face", "bz_face"]
+        out["per_box_loop_fp%d" % prec] = {
+            "ms": loop_ms, "boxes": nloop, "boxes_failed": nfail, "boxes_per_s": nloop / (loop_ms / 1e3),
+            "cell_updates_per_s": sample_cells_steps / (loop_ms / 1e3),
+            "batch_rel_l1_max_over_sample": {names[k]: v for k, v in l1.items()},
+            "timing": "host wall clock around each box's step loop (device synchronised)"}
+        out["speedup_vs_fp%d_loop" % prec] = out["batch"]["boxes_per_s"] / out["per_box_loop_fp%d" % prec]["boxes_per_s"]
+    return out
+
+
+# ----------------------------------------------------------------- serving loop
+def run_served(a, local):
+    """Poisson stream of box-solve requests (edges {32,64,96,128,192} weighted
+    0.35/0.30/0.20/0.10/0.05, steps U[20,200], Roe or HLLD, |B0| U[0.1,2],
+    Mach U[0.5,5], forcing on) served by imhd_server with continuous batching
+    under the HBM budget; boxes/s, cell-updates/s and p50/p99 latency from
+    submission to the result in host memory.  The first requests of the same
+    stream are also served one at a time by the plain per-box loop."""
+    import threading
+
+    import torch
+    from isothermal_mhd_b200 import Box, ImhdError, driver, workloads
+    from isothermal_mhd_b200.server import Server
+
+    stream_ = workloads.request_stream(a.served, rate=a.rate, seed=a.seed + 1)
+    specs = stream_.specs
+    srv = Server(precision=32, hbm_budget=a.hbm_budget, steps_per_round=4, device=local)
+    # warm-up: kernels loaded, first graph captured
+    warm = [srv.submit(workloads.BoxSpec(n=16, b0=(0.5, 0, 0), mach=1.0, steps=3, seed=1, riemann=r))
+            for r in ("roe", "hlld")]
+    for rid in warm:
+        while srv.poll(rid, fetch=True)[0] != "done":
+            time.sleep(0.001)
+    ids = [None] * len(specs)
+    t_start = time.perf_counter()
+
+    def submitter():
+        for i, s in enumerate(specs):
+            dt = t_start + s.arrival - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids[i] = srv.submit(s)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    lat, wait_s, failed = {}, {}, []
+    t_last = t_start
+    while len(lat) < len(specs):
+        for i in range(len(specs)):
+            if i in lat or ids[i] is None:
+                continue
+            state, info, _ = srv.poll(ids[i], fetch=True)
+            if state in ("done", "failed"):
+                lat[i] = info["latency_s"]
+                wait_s[i] = info["queue_wait_s"]
+                t_last = time.perf_counter()
+                if state == "failed":
+                    failed.append(i)
+        time.sleep(0.002)
+    th.join()
+    stats = srv.stats()
+    srv.stop(drain=True)
+    srv.close()
+    elapsed = t_last - t_start
+    lats = np.array([lat[i] for i in range(len(specs))])
+    cells_steps = sum(s.cells * s.steps for s in specs)
+    out = {"workload": "%d requests, Poisson %.0f req/s, edges {32,64,96,128,192} p=0.35/0.30/0.20/0.10/0.05, "
+                       "steps U[20,200], Roe/HLLD 1:1, |B0| U[0.1,2], Mach U[0.5,5], FP32, forcing on, "
+                       "HBM budget %.0f GB" % (len(specs), a.rate, a.hbm_budget / 1e9),
+           "requests": len(specs), "requests_failed": len(failed), "elapsed_s": elapsed,
+           "arrival_span_s": specs[-1].arrival,
+           "boxes_per_s": len(specs) / elapsed, "cell_updates_per_s": cells_steps / elapsed,
+           "latency_s": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
+                         "mean": float(lats.mean()), "max": float(lats.max())},
+           "queue_wait_s": {"p50": float(np.percentile([wait_s[i] for i in wait_s], 50)),
+                            "p99": float(np.percentile([wait_s[i] for i in wait_s], 99))},
+           "server": stats}
+    # plain per-box loops over the first requests of the stream, one at a time
+    nloop = min(a.loop_sample or len(specs), len(specs), 64)
+    for prec in (64, 32):
+        tot = 0.0
+        nfail = 0
+        for s in specs[:nloop]:
+            kv, av, sv, af, sf = s.fields()
+            box = Box(s.n, precision=prec, riemann=s.riemann, npass=s.npass, cour=a.cour, edot=s.edot,
+                      dt_turb=s.dt_turb, device=local)
+            t0 = time.perf_counter()
+            box.init_uniform(1.0, s.b0)
+            box.fourier_field("velocity", kv, av, sv)
+            box.fourier_field("force", kv, af, sf)
+            dt0 = a.cour * box.dx / box.max_speed()
+            try:
+                driver.run(box, t_end=1e30, maxsteps=s.steps + 1, dt0=dt0, forcing="device", dt_turb=s.dt_turb,
+                           record_dt=False)
+            except ImhdError:
+                nfail += 1
+            box.download()
+            torch.cuda.synchronize()
+            tot += time.perf_counter() - t0
+            box.close()
+        out["per_box_loop_fp%d" % prec] = {
+            "requests": nloop, "requests_failed": nfail, "boxes_per_s": nloop / tot,
+            "cell_updates_per_s": sum(s.cells * s.steps for s in specs[:nloop]) / tot,
+            "timing": "host wall clock per request: build, step loop, download (one request at a time)"}
+        # the sample's mix differs from the stream's: compare the time each
+        # would take for the whole stream's work
+        sample_work = sum(s.cells * s.steps for s in specs[:nloop])
+        loop_time_stream = tot * cells_steps / sample_work
+        out["per_box_loop_fp%d" % prec]["est_s_for_stream"] = loop_time_stream
+        out["speedup_vs_fp%d_loop" % prec] = loop_time_stream / elapsed
+    return out
 
 
 # ----------------------------------------------------------------- CPU reference

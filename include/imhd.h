@@ -161,6 +161,12 @@ int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int res
  * host, e.g. the Ornstein-Uhlenbeck forcing of isothermal_mhd_b200.forcing. */
 int imhd_fourier_field(imhd_box* box, int target, const int* kvec, const double* amp, int nmodes, double scale);
 
+/* Uniform state: density rho, zero momentum, cell-centre and face field
+ * b0[3], passive scalars 0, as homogenous_stationary sets it up
+ * (init_domain_mod.f90:406-479); with imhd_fourier_field it builds a
+ * turbulence initial condition on the device without a host upload. */
+int imhd_init_uniform(imhd_box* box, double rho, const double* b0);
+
 /* ---- batches: many independent periodic boxes advanced together --------
  * All boxes of a batch share precision and device; sizes, Riemann solvers,
  * passive counts and physics parameters may differ.  Every kernel launch of a
@@ -184,11 +190,89 @@ int imhd_batch_schedule(imhd_batch* batch, int box, double t0, double t_end, lon
 int imhd_batch_run(imhd_batch* batch, int replays);
 /* Clock of one box: time, steps made, next dt, still running. */
 int imhd_batch_clock(imhd_batch* batch, int box, double* t, long long* steps, double* dt, int* active);
+int imhd_batch_init_uniform(imhd_batch* batch, int box, double rho, const double* b0);
 int imhd_batch_fourier_field(imhd_batch* batch, int box, int target, const int* kvec, const double* amp, int nmodes,
                              double scale);
 int imhd_batch_set_stream(imhd_batch* batch, void* stream);
 long long imhd_batch_launch_count(imhd_batch* batch);
 void imhd_batch_destroy(imhd_batch* batch);
+
+/* ---- serving: a request loop with continuous batching -------------------
+ * imhd_server_start launches a worker thread that owns one device.  Requests
+ * (a box solve: configuration, step count, initial condition, forcing) are
+ * queued by imhd_server_submit from any host thread; the worker admits them
+ * in arrival order while their device bytes fit hbm_budget_bytes (and, if
+ * max_resident_cells > 0, while the resident cells stay under it), builds
+ * each box on the device, and advances all resident boxes together with the
+ * batched step (per-box clocks as in imhd_batch_*).  Every steps_per_round
+ * replays it retires finished boxes (result copied to host memory, device
+ * memory freed) and admits waiting ones, so requests that arrive while others
+ * run join the running batch.  A box's result does not depend on what else
+ * is resident.  No reference counterpart (the reference runs one box per job).
+ *
+ * The initial condition of a request is a uniform state (rho, b0) plus the
+ * velocity of nmodes Fourier modes (imhd_fourier_field's convention, target
+ * velocity, amp_velocity scaled by scale_velocity); forcing != 0 drives the
+ * box on the reference schedule with the force field of amp_force scaled by
+ * scale_force (needs box.edot > 0).  dt0 <= 0 starts from COUR*dx/cmax of the
+ * initial state; t_end <= 0 means no end time (steps alone stop the box).
+ * box.precision and box.device are taken from the server. */
+typedef struct {
+    int device;
+    int precision;                /* 32 or 64 for every box of the server */
+    double hbm_budget_bytes;      /* device bytes of resident boxes */
+    long long max_resident_cells; /* 0: no limit besides the budget */
+    int steps_per_round;          /* graph replays between retire / admit passes */
+} imhd_server_config;
+
+typedef struct {
+    imhd_config box;
+    long long steps;
+    double t_end, dt0;
+    double rho;
+    double b0[3];
+    int nmodes;
+    const int* kvec;              /* 3 * nmodes */
+    const double* amp_velocity;   /* 6 * nmodes or NULL */
+    double scale_velocity;
+    const double* amp_force;      /* 6 * nmodes, used when forcing != 0 */
+    double scale_force;
+    int forcing;
+} imhd_request;
+
+#define IMHD_REQ_QUEUED 0
+#define IMHD_REQ_RUNNING 1
+#define IMHD_REQ_DONE 2
+#define IMHD_REQ_FAILED 3
+#define IMHD_REQ_CANCELLED 4
+#define IMHD_SERVER_NSTATS 16
+
+typedef struct imhd_server imhd_server;
+void imhd_server_default_config(imhd_server_config* cfg);
+int imhd_server_start(const imhd_server_config* cfg, imhd_server** server);
+/* Queue a request; *id names it in imhd_server_poll.  The arrays are copied. */
+int imhd_server_submit(imhd_server* server, const imhd_request* req, long long* id);
+/* State of a request (IMHD_REQ_*) and info[5] = {t, steps made, latency from
+ * submit to result on the host in s (-1 before), queue wait in s, status
+ * bits}.  When the request is done and any of q / bface / qpass is non-NULL,
+ * the result is copied there (layout of imhd_download with the request's
+ * ghost widths) and released: the id is unknown afterwards.  A failed
+ * request returns IMHD_E_PHYSICS with the reason in imhd_last_error. */
+int imhd_server_poll(imhd_server* server, long long id, int* state, double* q, double* bface, double* qpass,
+                     double* info);
+/* {queued, resident, admitted, completed, failed, graph replays, kernel
+ * launches, table rebuilds, resident bytes, peak resident bytes, peak
+ * resident boxes, then seconds the worker spent building admitted boxes,
+ * rebuilding the table and graph, stepping, reading clocks and retiring, and
+ * seconds the harvester spent downloading results}; n >= IMHD_SERVER_NSTATS.
+ * Finished boxes are downloaded by a second thread on a stream of their own
+ * while the step loop goes on; their memory counts against the budget until
+ * the download ends. */
+int imhd_server_stats(imhd_server* server, double* out, int n);
+/* Stop the worker: drain != 0 finishes every queued and running request
+ * first, drain == 0 cancels them.  Results stay pollable until destroy. */
+int imhd_server_stop(imhd_server* server, int drain);
+void imhd_server_destroy(imhd_server* server);
 
 /* One undriven time step, like imhd_step, for callers that cannot allocate
  * device memory: hosts that own every device buffer (pool allocators,

@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libimhd.so")
 
 IMHD_OK = 0
+IMHD_E_PHYSICS = 4
 ERRORS = {1: "IMHD_E_ARG", 2: "IMHD_E_CUDA", 3: "IMHD_E_NOMEM", 4: "IMHD_E_PHYSICS", 5: "IMHD_E_STATE"}
 S_FLOOR, S_NAN, S_ZERO_SPEED, S_FORCE = 1, 2, 4, 8
 
@@ -20,10 +21,12 @@ EXPORTS = (
     "imhd_default_config", "imhd_create", "imhd_upload", "imhd_download", "imhd_set_force",
     "imhd_step", "imhd_max_speed", "imhd_diagnostics", "imhd_status", "imhd_wave_speeds",
     "imhd_destroy", "imhd_last_error", "imhd_launch_count", "imhd_set_stream", "imhd_profile",
-    "imhd_stage_times", "imhd_step_static", "imhd_fourier_field",
+    "imhd_stage_times", "imhd_step_static", "imhd_fourier_field", "imhd_init_uniform",
     "imhd_batch_create", "imhd_batch_upload", "imhd_batch_set_force", "imhd_batch_download", "imhd_batch_schedule",
-    "imhd_batch_run", "imhd_batch_clock", "imhd_batch_fourier_field", "imhd_batch_set_stream",
+    "imhd_batch_run", "imhd_batch_clock", "imhd_batch_init_uniform", "imhd_batch_fourier_field", "imhd_batch_set_stream",
     "imhd_batch_launch_count", "imhd_batch_destroy",
+    "imhd_server_default_config", "imhd_server_start", "imhd_server_submit", "imhd_server_poll",
+    "imhd_server_stats", "imhd_server_stop", "imhd_server_destroy",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -39,6 +42,27 @@ class ImhdConfig(ctypes.Structure):
         ("edot", ctypes.c_double), ("dt_turb", ctypes.c_double),
         ("ng", ctypes.c_int), ("ng_pass", ctypes.c_int), ("device", ctypes.c_int),
     ]
+
+
+class ImhdServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_double),
+        ("max_resident_cells", ctypes.c_longlong), ("steps_per_round", ctypes.c_int),
+    ]
+
+
+class ImhdRequest(ctypes.Structure):
+    _fields_ = [
+        ("box", ImhdConfig), ("steps", ctypes.c_longlong), ("t_end", ctypes.c_double), ("dt0", ctypes.c_double),
+        ("rho", ctypes.c_double), ("b0", ctypes.c_double * 3), ("nmodes", ctypes.c_int),
+        ("kvec", ctypes.POINTER(ctypes.c_int)), ("amp_velocity", ctypes.POINTER(ctypes.c_double)),
+        ("scale_velocity", ctypes.c_double), ("amp_force", ctypes.POINTER(ctypes.c_double)),
+        ("scale_force", ctypes.c_double), ("forcing", ctypes.c_int),
+    ]
+
+
+REQ_STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+SERVER_NSTATS = 16
 
 
 class ImhdError(RuntimeError):
@@ -97,6 +121,10 @@ def lib():
         ip = ctypes.POINTER(ctypes.c_int)
         L.imhd_fourier_field.argtypes = [vp, i, ip, dp, i, d]
         L.imhd_fourier_field.restype = i
+        L.imhd_init_uniform.argtypes = [vp, d, dp]
+        L.imhd_init_uniform.restype = i
+        L.imhd_batch_init_uniform.argtypes = [vp, i, d, dp]
+        L.imhd_batch_init_uniform.restype = i
         L.imhd_batch_create.argtypes = [ctypes.POINTER(ImhdConfig), i, ctypes.POINTER(vp)]
         L.imhd_batch_create.restype = i
         for name in ("imhd_batch_upload", "imhd_batch_download"):
@@ -118,6 +146,20 @@ def lib():
         L.imhd_batch_launch_count.restype = ctypes.c_longlong
         L.imhd_batch_destroy.argtypes = [vp]
         L.imhd_batch_destroy.restype = None
+        L.imhd_server_default_config.argtypes = [ctypes.POINTER(ImhdServerConfig)]
+        L.imhd_server_default_config.restype = None
+        L.imhd_server_start.argtypes = [ctypes.POINTER(ImhdServerConfig), ctypes.POINTER(vp)]
+        L.imhd_server_start.restype = i
+        L.imhd_server_submit.argtypes = [vp, ctypes.POINTER(ImhdRequest), ctypes.POINTER(ctypes.c_longlong)]
+        L.imhd_server_submit.restype = i
+        L.imhd_server_poll.argtypes = [vp, ctypes.c_longlong, ip, dp, dp, dp, dp]
+        L.imhd_server_poll.restype = i
+        L.imhd_server_stats.argtypes = [vp, dp, i]
+        L.imhd_server_stats.restype = i
+        L.imhd_server_stop.argtypes = [vp, i]
+        L.imhd_server_stop.restype = i
+        L.imhd_server_destroy.argtypes = [vp]
+        L.imhd_server_destroy.restype = None
         _lib = L
     return _lib
 

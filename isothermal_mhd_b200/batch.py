@@ -12,7 +12,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import ImhdConfig, check, lib
+from ._lib import IMHD_E_PHYSICS, ImhdConfig, check, lib
 from .box import RIEMANN, _dptr
 
 
@@ -98,8 +98,16 @@ class Batch:
         s = ctypes.c_longlong()
         dt = ctypes.c_double()
         a = ctypes.c_int()
-        check(lib().imhd_batch_clock(self._h, i, ctypes.byref(t), ctypes.byref(s), ctypes.byref(dt), ctypes.byref(a)))
-        return {"t": t.value, "steps": s.value, "dt": dt.value, "active": bool(a.value)}
+        rc = lib().imhd_batch_clock(self._h, i, ctypes.byref(t), ctypes.byref(s), ctypes.byref(dt), ctypes.byref(a))
+        if rc not in (0, IMHD_E_PHYSICS):
+            check(rc)
+        # failed: the box stopped on a physics error (NaN or zero max speed)
+        return {"t": t.value, "steps": s.value, "dt": dt.value, "active": bool(a.value),
+                "failed": rc == IMHD_E_PHYSICS}
+
+    def init_uniform(self, i, rho=1.0, b0=(0.0, 0.0, 0.0)):
+        b = np.ascontiguousarray(b0, dtype=np.float64)
+        check(lib().imhd_batch_init_uniform(self._h, i, float(rho), _dptr(b)))
 
     def fourier_field(self, i, target, kvec, amp, scale):
         kv = np.ascontiguousarray(kvec, dtype=np.int32).reshape(-1, 3)

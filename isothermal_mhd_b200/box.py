@@ -156,6 +156,11 @@ class Box:
         ``torch.cuda.current_stream().cuda_stream``); None restores the box's own."""
         check(lib().imhd_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
 
+    def init_uniform(self, rho=1.0, b0=(0.0, 0.0, 0.0)):
+        """Density rho, zero momentum, uniform field b0, passive scalars 0."""
+        b = np.ascontiguousarray(b0, dtype=np.float64)
+        check(lib().imhd_init_uniform(self._h, float(rho), _dptr(b)))
+
     def fourier_field(self, target, kvec, amp, scale):
         """Fill from Fourier modes on the device: target "velocity" adds
         rho * scale * v to the momentum, "force" sets the force field to scale * v

@@ -32,6 +32,7 @@ UNITS = {
     "imhd_capi.cu": [],
     "imhd_static.cu": [],
     "imhd_batch.cu": [],
+    "imhd_server.cu": [],
 }
 HEADERS = ["imhd_physics.cuh", "imhd_physics_fast.cuh", "imhd_types.cuh", "imhd_table.h", "imhd_kernels.cuh", "imhd_launch.cuh"]
 

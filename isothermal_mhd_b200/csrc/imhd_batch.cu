@@ -26,6 +26,7 @@ template <class T> cudaError_t run_from_f64(cudaStream_t, const double*, void*, 
 template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, int);
 template <class T> cudaError_t run_ou_field(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int,
                                             double);
+template <class T> cudaError_t run_init_uniform(cudaStream_t, const BoxRec&, int, double, const double*);
 const char* set_last_error(int code, const char* msg);
 }  // namespace imhd
 
@@ -45,6 +46,7 @@ struct imhd_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool graph_dirty = true;
+    long long graph_kernels = 0;        // kernel launches of one replay
 };
 
 namespace {
@@ -116,19 +118,7 @@ int bdownload_field(imhd_batch* x, int box, const void* src, double* h, int ng) 
     return IMHD_OK;
 }
 
-void bghost_fill(const imhd_config& c, double* h, int ng) {
-    if (ng == 0) return;
-    long Px = c.nx + 2 * ng, Py = c.ny + 2 * ng, Pz = c.nz + 2 * ng;
-    auto wrap = [](long i, long n) { i %= n; return i < 0 ? i + n : i; };
-    for (long k = 0; k < Pz; ++k)
-        for (long j = 0; j < Py; ++j)
-            for (long i = 0; i < Px; ++i) {
-                bool in = i >= ng && i < ng + c.nx && j >= ng && j < ng + c.ny && k >= ng && k < ng + c.nz;
-                if (in) continue;
-                long ii = wrap(i - ng, c.nx) + ng, jj = wrap(j - ng, c.ny) + ng, kk = wrap(k - ng, c.nz) + ng;
-                h[i + Px * (j + Py * k)] = h[ii + Px * (jj + Py * kk)];
-            }
-}
+void bghost_fill(const imhd_config& c, double* h, int ng) { imhd::host_ghost_fill(c.nx, c.ny, c.nz, h, ng); }
 
 int read_scalars(imhd_batch* x, int box, imhd::Scalars& s) {
     BCK(cudaMemcpyAsync(&s, x->rec[box].sc, sizeof(s), cudaMemcpyDeviceToHost, x->st));
@@ -142,6 +132,23 @@ int write_scalars(imhd_batch* x, int box, const imhd::Scalars& s) {
 }
 
 bool check_box(imhd_batch* x, int box) { return x && box >= 0 && box < (int)x->rec.size(); }
+
+// Box `box` of the batch alone, its record (current state first) in the
+// kernel parameters: per-box operations launch over that box only.
+imhd::BatchDev one_box(const imhd_batch* x, int box, int cur) {
+    imhd::BatchDev d = x->b;
+    const imhd::BoxRec& r = x->rec[box];
+    d.a.use_one = 1;
+    d.a.one = r;
+    d.a.one.S[0] = r.S[cur];
+    d.a.one.S[1] = r.S[cur ^ 1];
+    d.a.one.active = 1;
+    d.a.nbox = 1;
+    for (int k = 0; k < imhd::kKinds; ++k) d.totals[k] = (int)imhd::blocks_of(r, k, x->esz);
+    d.prof = false;
+    d.launches = 0;
+    return d;
+}
 
 }  // namespace
 
@@ -181,12 +188,9 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         if ((size_t)x->rec[i].n > maxn) maxn = x->rec[i].n;
         forcing = forcing || c.edot > 0.0;
     }
-    std::vector<int> prefix;
-    if (!imhd::build_prefix(x->rec, x->esz, prefix, x->b)) { delete x; return bfail(IMHD_E_ARG, "batch too large for one launch"); }
-    std::vector<std::vector<int>> b2b;
-    imhd::build_blk2box(prefix, nbox, x->b, b2b);
-    size_t tab = imhd::align256(sizeof(imhd::BoxRec) * nbox) + imhd::align256(prefix.size() * sizeof(int));
-    for (int k = 0; k < imhd::kKinds; ++k) tab += imhd::align256(b2b[k].size() * sizeof(int) + 4);
+    imhd::TablePlan plan;
+    if (!imhd::plan_table(x->rec, x->esz, x->b, plan)) { delete x; return bfail(IMHD_E_ARG, "batch too large for one launch"); }
+    size_t tab = plan.bytes;
     bool ok = cudaStreamCreateWithFlags(&x->st, cudaStreamNonBlocking) == cudaSuccess;
     ok = ok && cudaMalloc(&x->pool, total) == cudaSuccess;
     ok = ok && cudaMalloc(&x->table, tab) == cudaSuccess;
@@ -209,20 +213,7 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         std::memset(&init, 0, sizeof(init));
         BCK(cudaMemcpyAsync(x->rec[i].sc, &init, sizeof(init), cudaMemcpyHostToDevice, x->st));
     }
-    BCK(cudaMemcpyAsync(x->table, x->rec.data(), sizeof(imhd::BoxRec) * nbox, cudaMemcpyHostToDevice, x->st));
-    size_t off = imhd::align256(sizeof(imhd::BoxRec) * nbox);
-    BCK(cudaMemcpyAsync((char*)x->table + off, prefix.data(), prefix.size() * sizeof(int), cudaMemcpyHostToDevice, x->st));
-    x->b.a.boxes = (imhd::BoxRec*)x->table;
-    x->b.a.prefix = (const int*)((char*)x->table + off);
-    off += imhd::align256(prefix.size() * sizeof(int));
-    for (int k = 0; k < imhd::kKinds; ++k) {
-        if (!b2b[k].empty())
-            BCK(cudaMemcpyAsync((char*)x->table + off, b2b[k].data(), b2b[k].size() * sizeof(int), cudaMemcpyHostToDevice,
-                                x->st));
-        x->b.a.blk2box[k] = (const int*)((char*)x->table + off);
-        off += imhd::align256(b2b[k].size() * sizeof(int) + 4);
-    }
-    BCK(cudaStreamSynchronize(x->st));
+    BCK(imhd::upload_table(x->table, x->rec, plan, x->st, x->b.a));
     x->b.a.use_one = 0;
     x->b.drive_mode = forcing ? 2 : 0;
     *out = x;
@@ -315,7 +306,9 @@ int imhd_batch_schedule(imhd_batch* x, int box, double t0, double t_end, long lo
         // COUR*dx/cmax of the uploaded state (get_max_speed_vanleer without smax)
         for (int k = 0; k < imhd::kSlots; ++k) s.cfl_slots[k] = 0ull;
         if ((rc = write_scalars(x, box, s))) return rc;
-        BCK(b64(x) ? imhd::run_max_speed<double>(x->b) : imhd::run_max_speed<float>(x->b));
+        imhd::BatchDev d = one_box(x, box, s.cur);
+        BCK(b64(x) ? imhd::run_max_speed<double>(d) : imhd::run_max_speed<float>(d));
+        x->b.launches += d.launches;
         if ((rc = read_scalars(x, box, s))) return rc;
         double m = 0.0;
         for (int k = 0; k < imhd::kSlots; ++k) {
@@ -353,7 +346,10 @@ int imhd_batch_run(imhd_batch* x, int replays) {
         if (x->exec) { cudaGraphExecDestroy(x->exec); x->exec = nullptr; }
         if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
         BCK(cudaStreamBeginCapture(x->st, cudaStreamCaptureModeThreadLocal));
+        const long long before = x->b.launches;
         cudaError_t e = b64(x) ? imhd::run_step<double>(x->b, 1) : imhd::run_step<float>(x->b, 1);
+        x->graph_kernels = x->b.launches - before;    // kernels per replay
+        x->b.launches = before;
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(x->st, &g);
         if (e != cudaSuccess || e2 != cudaSuccess) {
@@ -365,7 +361,10 @@ int imhd_batch_run(imhd_batch* x, int replays) {
         BCK(cudaGraphInstantiate(&x->exec, x->graph, 0));
         x->graph_dirty = false;
     }
-    for (int r = 0; r < replays; ++r) BCK(cudaGraphLaunch(x->exec, x->st));
+    for (int r = 0; r < replays; ++r) {
+        BCK(cudaGraphLaunch(x->exec, x->st));
+        x->b.launches += x->graph_kernels;
+    }
     BCK(cudaStreamSynchronize(x->st));
     return IMHD_OK;
 }
@@ -380,7 +379,8 @@ int imhd_batch_clock(imhd_batch* x, int box, double* t, long long* steps, double
     if (steps) *steps = s.steps_done;
     if (dt) *dt = s.dt;
     if (active) *active = s.active;
-    if (s.status & (IMHD_S_ZERO_SPEED | IMHD_S_FORCE)) return bfail(IMHD_E_PHYSICS, "box stopped on a physics error");
+    if (s.status & (IMHD_S_NAN | IMHD_S_ZERO_SPEED | IMHD_S_FORCE))
+        return bfail(IMHD_E_PHYSICS, "box stopped on a physics error (non-finite state, zero max speed or forcing)");
     return IMHD_OK;
 }
 
@@ -396,6 +396,20 @@ int imhd_batch_set_stream(imhd_batch* x, void* stream) {
 long long imhd_batch_launch_count(imhd_batch* x) { return x ? x->b.launches : 0; }
 
 // Fill one box from a sum of Fourier modes (see imhd_ou_field in imhd.h).
+int imhd_batch_init_uniform(imhd_batch* x, int box, double rho, const double* b0) {
+    if (!check_box(x, box) || !b0) return bfail(IMHD_E_ARG, "bad box index or null b0");
+    if (!(rho > 0.0)) return bfail(IMHD_E_ARG, "rho must be positive");
+    BCK(cudaSetDevice(x->device));
+    imhd::Scalars s;
+    int rc = read_scalars(x, box, s);
+    if (rc) return rc;
+    BCK(b64(x) ? imhd::run_init_uniform<double>(x->st, x->rec[box], s.cur, rho, b0)
+               : imhd::run_init_uniform<float>(x->st, x->rec[box], s.cur, rho, b0));
+    x->b.launches += 1;
+    BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
 int imhd_batch_fourier_field(imhd_batch* x, int box, int target, const int* kvec, const double* amp, int nmodes,
                              double scale) {
     if (!check_box(x, box) || nmodes < 0 || (nmodes > 0 && (!kvec || !amp))) return bfail(IMHD_E_ARG, "bad argument");

@@ -20,6 +20,7 @@ template <class T> cudaError_t run_from_f64(cudaStream_t, const double*, void*, 
 template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, int);
 template <class T> cudaError_t run_ou_field(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int,
                                             double);
+template <class T> cudaError_t run_init_uniform(cudaStream_t, const BoxRec&, int, double, const double*);
 }  // namespace imhd
 
 struct imhd_box {
@@ -438,6 +439,16 @@ int imhd_wave_speeds(imhd_box* x, double* smax, double* delv_max) {
 }
 
 long long imhd_launch_count(imhd_box* x) { return x ? x->b.launches : 0; }
+
+int imhd_init_uniform(imhd_box* x, double rho, const double* b0) {
+    if (!x || !b0) return fail(IMHD_E_ARG, "null argument");
+    if (!(rho > 0.0)) return fail(IMHD_E_ARG, "rho must be positive");
+    CK(cudaSetDevice(x->cfg.device));
+    CK(is64(x) ? imhd::run_init_uniform<double>(x->b.st, x->rec, x->cur, rho, b0)
+               : imhd::run_init_uniform<float>(x->b.st, x->rec, x->cur, rho, b0));
+    x->b.launches += 1;
+    return sync_and_check(x);
+}
 
 int imhd_fourier_field(imhd_box* x, int target, const int* kvec, const double* amp, int nmodes, double scale) {
     if (!x || nmodes < 0 || (nmodes > 0 && (!kvec || !amp))) return fail(IMHD_E_ARG, "bad argument");

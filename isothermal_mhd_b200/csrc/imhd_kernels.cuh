@@ -433,7 +433,6 @@ template <class T, bool ONE>
 __global__ void __launch_bounds__(kBX) k_corner_emf(BatchArgs ba, int half_step_state) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
-    Scalars* scb = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
     const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
@@ -964,6 +963,22 @@ static __global__ void k_batch_begin(BatchArgs ba) {
     sc->drive = drive;
 }
 
+// Clocks of every box of a table, kClockWords doubles per box:
+// t, steps made, running flag, current buffer, status bits, next dt.
+constexpr int kClockWords = 6;
+static __global__ void k_clocks(BatchArgs ba, double* __restrict__ out) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= ba.nbox) return;
+    const Scalars* sc = box_at(ba, b).sc;
+    double* o = out + (size_t)b * kClockWords;
+    o[0] = sc->t;
+    o[1] = (double)sc->steps_done;
+    o[2] = (double)sc->active;
+    o[3] = (double)sc->cur;
+    o[4] = (double)sc->status;
+    o[5] = sc->dt;
+}
+
 // cell fast-speed maximum of a state (imhd_max_speed)
 template <class T, bool ONE>
 __global__ void __launch_bounds__(kBX) k_cfl(BatchArgs ba) {
@@ -993,7 +1008,6 @@ template <class T, bool ONE>
 __global__ void __launch_bounds__(kRedThreads) k_diag(BatchArgs ba) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindRed, local);
-    const Scalars* sc = rp.sc;
     const Dims dm = dims_of(rp);
     const T* __restrict__ S = (const T*)rp.S[0];
     double* __restrict__ partials = rp.partials;
@@ -1070,7 +1084,7 @@ __global__ void __launch_bounds__(kBX) k_fourier_field(BoxRec r, int cur, int ta
         for (int d = 0; d < 3; ++d) v[d] += 2.0 * (amp[6 * m + 2 * d] * co - amp[6 * m + 2 * d + 1] * s);
     }
     if (target == 0) {
-        T* S = (T*)r.S[cur];
+        T* S = (T*)(cur ? r.S[1] : r.S[0]);
         double rho = (double)S[c];
 #pragma unroll
         for (int d = 0; d < 3; ++d) S[(size_t)(1 + d) * r.n + c] = (T)((double)S[(size_t)(1 + d) * r.n + c] + rho * scale * v[d]);
@@ -1079,6 +1093,21 @@ __global__ void __launch_bounds__(kBX) k_fourier_field(BoxRec r, int cur, int ta
 #pragma unroll
         for (int d = 0; d < 3; ++d) D[(size_t)d * r.n + c] = (T)(scale * v[d]);
     }
+}
+
+// Uniform state of S[cur]: density rho, zero momentum, cell-centre and face
+// field b0, passive scalars 0 (the homogenous_stationary set-up of
+// init_domain_mod.f90:406-479 with a uniform field).
+template <class T>
+__global__ void __launch_bounds__(kBX) k_init_uniform(BoxRec r, int cur, double rho, double bx, double by, double bz) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= r.n) return;
+    T* S = (T*)(cur ? r.S[1] : r.S[0]);
+    const size_t n = (size_t)r.n;
+    const T v[10] = {(T)rho, T(0), T(0), T(0), (T)bx, (T)by, (T)bz, (T)bx, (T)by, (T)bz};
+#pragma unroll
+    for (int f = 0; f < 10; ++f) S[f * n + c] = v[f];
+    for (int p = 0; p < r.npass; ++p) S[(10 + p) * n + c] = T(0);
 }
 
 // ============================================================ host transfer

@@ -218,6 +218,20 @@ cudaError_t run_ou_field(cudaStream_t st, const BoxRec& r, int cur, int target, 
     return cudaGetLastError();
 }
 
+template <class T>
+cudaError_t run_clocks(BatchDev& b, double* out) {
+    k_clocks<<<(b.a.nbox + 127) / 128, 128, 0, b.st>>>(b.a, out);
+    b.launches += 1;
+    return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t run_init_uniform(cudaStream_t st, const BoxRec& r, int cur, double rho, const double* b0) {
+    int blocks = (r.n + kBX - 1) / kBX;
+    k_init_uniform<T><<<blocks, kBX, 0, st>>>(r, cur, rho, b0[0], b0[1], b0[2]);
+    return cudaGetLastError();
+}
+
 }  // namespace imhd
 
 #define IMHD_INSTANTIATE(T)                                                        \
@@ -230,4 +244,6 @@ cudaError_t run_ou_field(cudaStream_t st, const BoxRec& r, int cur, int target, 
     template cudaError_t run_to_f64<T>(cudaStream_t, const void*, double*, int);   \
     template cudaError_t run_ou_field<T>(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int, \
                                          double);                                  \
+    template cudaError_t run_init_uniform<T>(cudaStream_t, const BoxRec&, int, double, const double*); \
+    template cudaError_t run_clocks<T>(BatchDev&, double*);                       \
     }

@@ -12,6 +12,7 @@
 namespace imhd {
 
 inline int ceil_div(long a, long b) { return (int)((a + b - 1) / b); }
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 inline bool row_capable(int nx, size_t esz) { return 13 * (size_t)nx * esz <= kRowSmemMax; }
 
@@ -81,6 +82,65 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
     return true;
 }
 
+// Host side of a device table: block prefixes, block -> box lists and the
+// device bytes of the whole table (records | prefix | one list per kind).
+struct TablePlan {
+    std::vector<int> prefix;
+    std::vector<std::vector<int>> b2b;
+    size_t bytes = 0;
+};
+
+inline bool plan_table(const std::vector<BoxRec>& recs, size_t esz, BatchDev& bd, TablePlan& tp) {
+    if (!build_prefix(recs, esz, tp.prefix, bd)) return false;
+    build_blk2box(tp.prefix, (int)recs.size(), bd, tp.b2b);
+    tp.bytes = align256(sizeof(BoxRec) * recs.size()) + align256(tp.prefix.size() * sizeof(int));
+    for (int k = 0; k < kKinds; ++k) tp.bytes += align256(tp.b2b[k].size() * sizeof(int) + 4);
+    return true;
+}
+
+// Copy a planned table to `dev` (tp.bytes of device memory) and point the
+// launch arguments at it.  The host vectors are pageable, so the copies are
+// complete when this returns.
+inline cudaError_t upload_table(void* dev, const std::vector<BoxRec>& recs, const TablePlan& tp, cudaStream_t st,
+                                BatchArgs& a) {
+    cudaError_t e = cudaMemcpyAsync(dev, recs.data(), sizeof(BoxRec) * recs.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    size_t off = align256(sizeof(BoxRec) * recs.size());
+    e = cudaMemcpyAsync((char*)dev + off, tp.prefix.data(), tp.prefix.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    a.boxes = (BoxRec*)dev;
+    a.prefix = (const int*)((char*)dev + off);
+    off += align256(tp.prefix.size() * sizeof(int));
+    for (int k = 0; k < kKinds; ++k) {
+        if (!tp.b2b[k].empty()) {
+            e = cudaMemcpyAsync((char*)dev + off, tp.b2b[k].data(), tp.b2b[k].size() * sizeof(int),
+                                cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return e;
+        }
+        a.blk2box[k] = (const int*)((char*)dev + off);
+        off += align256(tp.b2b[k].size() * sizeof(int) + 4);
+    }
+    a.nbox = (int)recs.size();
+    a.use_one = 0;
+    return cudaStreamSynchronize(st);
+}
+
+// Periodic ghost layers of a padded host field whose interior is filled
+// (boundary_conditions_mod.f90:137-231 on the host side of the boundary).
+inline void host_ghost_fill(int nx, int ny, int nz, double* h, int ng) {
+    if (ng == 0) return;
+    long Px = nx + 2 * ng, Py = ny + 2 * ng, Pz = nz + 2 * ng;
+    auto wrap = [](long i, long n) { i %= n; return i < 0 ? i + n : i; };
+    for (long k = 0; k < Pz; ++k)
+        for (long j = 0; j < Py; ++j)
+            for (long i = 0; i < Px; ++i) {
+                bool in = i >= ng && i < ng + nx && j >= ng && j < ng + ny && k >= ng && k < ng + nz;
+                if (in) continue;
+                long ii = wrap(i - ng, nx) + ng, jj = wrap(j - ng, ny) + ng, kk = wrap(k - ng, nz) + ng;
+                h[i + Px * (j + Py * k)] = h[ii + Px * (jj + Py * kk)];
+            }
+}
+
 // Fill the geometry fields of a box record from its configuration.
 inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, double cs, double cour, double edot,
                      double dt_turb) {
@@ -105,7 +165,6 @@ inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, 
 
 // Device bytes of one box's buffers (state x2, fluxes, EMFs, half-step
 // scalars, boundary planes, partial sums, scalars), each 256-byte aligned.
-inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 inline size_t box_bytes(const BoxRec& r, size_t esz, bool with_force) {
     size_t n = (size_t)r.n, nf = 10 + (size_t)r.npass;
     size_t b = 2 * align256(nf * n * esz) + align256(18 * n * esz) + align256(3 * n * esz);

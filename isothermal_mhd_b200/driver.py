@@ -27,7 +27,8 @@ def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, r
     maxsteps follows the reference's counter: tsteps starts at 1 and the loop
     runs while tsteps < maxsteps, so maxsteps = N + 1 gives N steps.
     `forcing` is a callable returning the next delv field (3, nz+2g, ny+2g,
-    nx+2g) or None for an undriven run.
+    nx+2g), "device" for a force field already on the device (set by
+    Box.fourier_field; every drive reuses it), or None for an undriven run.
     """
     rec = RunRecord(t=t0)
     t_sim = t0
@@ -35,7 +36,8 @@ def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, r
     my_dt = dt0
     dt_turb = box.cfg.dt_turb if dt_turb is None else dt_turb
     t_turb = t_sim + dt_turb
-    if forcing is not None:
+    host_field = callable(forcing)
+    if host_field:
         box.set_force(forcing())
     while t_sim < t_end and tsteps < maxsteps:
         t_old = t_sim
@@ -51,7 +53,7 @@ def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, r
             rec.drive_steps.append(tsteps)
         t_sim = t_sim + my_dt
         tsteps += 1
-        if drive_next and forcing is not None:
+        if drive_next and host_field:
             box.set_force(forcing())
         my_dt = min(t_end - t_sim, dt_new)
         if on_step is not None:

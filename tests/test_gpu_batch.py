@@ -100,3 +100,23 @@ def test_schedule_without_dt0_uses_cfl_of_the_state():
         bt.upload(0, ic[0], ic[1])
         bt.schedule(0, 3, dt0=0.0)
         assert bt.clock(0)["dt"] == dt_expect
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_init_uniform_equals_uploaded_uniform_state(precision):
+    n = (12, 10, 8)
+    b0 = (0.3, -0.2, 0.7)
+    q, b, p = problems.uniform_box(n, rho=1.5, b0=b0, npass=2)
+    p[...] = 0.0
+    with Box(n, precision=precision, riemann="hlld", npass=2) as box:
+        box.init_uniform(1.5, b0)
+        qg, bg, pg = box.download()
+    np.testing.assert_array_equal(qg, q.astype(np.float32) if precision == 32 else q)
+    np.testing.assert_array_equal(bg, b.astype(np.float32) if precision == 32 else b)
+    np.testing.assert_array_equal(pg, p)
+    with Batch([make_config(16, precision=precision, npass=0), make_config(n, precision=precision, npass=2)]) as bt:
+        bt.init_uniform(1, 1.5, b0)
+        qb, bb, pb = bt.download(1)
+    np.testing.assert_array_equal(qb, qg)
+    np.testing.assert_array_equal(bb, bg)
+    np.testing.assert_array_equal(pb, pg)
