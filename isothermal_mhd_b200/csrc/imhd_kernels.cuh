@@ -70,6 +70,27 @@ __device__ __forceinline__ void decode_cell(int local, const Dims& dm, int& i, i
     }
 }
 
+// kKindCellZ decomposition: ceil(nx/kBX) blocks per (j, z segment); the
+// thread's column is k0 <= k < k1 (a single box launches a 3D grid
+// (nbx, ny, nseg))
+template <bool ONE>
+__device__ __forceinline__ void decode_cellz(int local, const Dims& dm, int& i, int& j, int& k0, int& k1) {
+    int seg;
+    if constexpr (ONE) {
+        i = (int)(blockIdx.x * kBX + threadIdx.x);
+        j = (int)blockIdx.y;
+        seg = (int)blockIdx.z;
+    } else {
+        int nbx = (dm.nx + kBX - 1) / kBX;
+        int bx = local % nbx, rest = local / nbx;
+        j = rest % dm.ny;
+        seg = rest / dm.ny;
+        i = bx * kBX + (int)threadIdx.x;
+    }
+    k0 = seg * kSegZ;
+    k1 = min(k0 + kSegZ, dm.nz);
+}
+
 __device__ __forceinline__ int wrap_up(int i, int n) { return (i + 1 == n) ? 0 : i + 1; }
 __device__ __forceinline__ int wrap_dn(int i, int n) { return (i == 0) ? n - 1 : i - 1; }
 __device__ __forceinline__ int wrap_any(int i, int n) { i %= n; return i < 0 ? i + n : i; }
@@ -429,23 +450,43 @@ __device__ __forceinline__ void upwind_pair(T v, T L14, T R14, T L34, T R34, T& 
     else { o14 = T(0.5) * (L14 + R14); o34 = T(0.5) * (L34 + R34); }
 }
 
+// One cell's cell-centre EMF and velocity, from its 7 conserved fields.
+template <class T>
+struct CellEV {
+    T ex, ey, ez;    // ecc3
+    T ux, uy, uz;    // m / rho, as face_v divides
+};
+template <class T>
+__device__ __forceinline__ CellEV<T> cell_ev(const T* __restrict__ S, int n, int c) {
+    CellEV<T> o;
+    ecc3(S, n, c, o.ex, o.ey, o.ez);
+    const T r = fld(S, 0, n)[c];
+    o.ux = fld(S, 1, n)[c] / r;
+    o.uy = fld(S, 2, n)[c] / r;
+    o.uz = fld(S, 3, n)[c] / r;
+    return o;
+}
+
+// A thread walks a column of kSegZ cells along z.  The cell-centre EMFs and
+// velocities of plane k+1 computed at one step are those of plane k at the
+// next, and so are the z-face EMFs read at k+1, so each is loaded and
+// computed once per column instead of once per neighbour.
 template <class T, bool ONE>
-__global__ void __launch_bounds__(kBX) k_corner_emf(BatchArgs ba, int half_step_state) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(BatchArgs ba, int half_step_state) {
     int local;
-    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
     const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
     const T* __restrict__ F = (const T*)rp.F;
     T* __restrict__ E = (T*)rp.E;
-    int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
+    int i, j, k0, k1;
+    decode_cellz<ONE>(local, dm, i, j, k0, k1);
     if (i >= dm.nx) return;
     const int n = dm.n;
-    int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny), kp = wrap_up(k, dm.nz);
-    auto C = [&](int a, int b, int c) { return a + dm.nx * (b + dm.ny * c); };
-    int c000 = C(i, j, k), c100 = C(ip, j, k), c010 = C(i, jp, k), c001 = C(i, j, kp);
-    int c110 = C(ip, jp, k), c101 = C(ip, j, kp), c011 = C(i, jp, kp);
+    const int plane = dm.nx * dm.ny;
+    const int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny);
+    const int r000 = i + dm.nx * j, r100 = ip + dm.nx * j, r010 = i + dm.nx * jp, r110 = ip + dm.nx * jp;
     // face EMFs: E_{t2} = -F_bt1, E_{t1} = F_bt2 of sweep D
     const T* Fx_bt1 = F + (size_t)4 * n;    // x sweep: -Ez at x-face
     const T* Fx_bt2 = F + (size_t)5 * n;    //           Ey at x-face
@@ -453,73 +494,89 @@ __global__ void __launch_bounds__(kBX) k_corner_emf(BatchArgs ba, int half_step_
     const T* Fy_bt2 = F + (size_t)11 * n;   //           Ez at y-face
     const T* Fz_bt1 = F + (size_t)16 * n;   // z sweep: -Ey at z-face
     const T* Fz_bt2 = F + (size_t)17 * n;   //           Ex at z-face
-    T vx = face_v(S, n, c000, c100, 0);
-    T vy = face_v(S, n, c000, c010, 1);
-    T vz = face_v(S, n, c000, c001, 2);
-    T e000x, e000y, e000z, e100x, e100y, e100z, e010x, e010y, e010z, e001x, e001y, e001z;
-    ecc3(S, n, c000, e000x, e000y, e000z);
-    ecc3(S, n, c100, e100x, e100y, e100z);
-    ecc3(S, n, c010, e010x, e010y, e010z);
-    ecc3(S, n, c001, e001x, e001y, e001z);
-    // Ez at (i+1/2, j+1/2, k)
-    {
-        T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
-        T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
-        T E33_000 = e000z, E33_100 = e100z, E33_010 = e010z, E33_110 = ecc(S, n, c110, 2);
-        T dyL14 = T(2) * (E32_000 - E33_000);
-        T dyR14 = T(2) * (E32_100 - E33_100);
-        T dyL34 = T(2) * (E33_010 - E32_000);
-        T dyR34 = T(2) * (E33_110 - E32_100);
-        T dy1214, dy1234;
-        upwind_pair(vx, dyL14, dyR14, dyL34, dyR34, dy1214, dy1234);
-        T dxL14 = T(2) * (E31_000 - E33_000);
-        T dxR14 = T(2) * (E31_010 - E33_010);
-        T dxL34 = T(2) * (E33_100 - E31_000);
-        T dxR34 = T(2) * (E33_110 - E31_010);
-        T dx1412, dx3412;
-        upwind_pair(vy, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
-        E[(size_t)2 * n + c000] = T(0.25) * (E31_000 + E31_010 + E32_000 + E32_100) +
-                                  T(0.125) * ((dy1214 - dy1234) + (dx1412 - dx3412));
-    }
-    // Ey at (i+1/2, j, k+1/2)
-    {
-        T E21_000 = Fx_bt2[c000], E21_001 = Fx_bt2[c001];
-        T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
-        T E23_000 = e000y, E23_100 = e100y, E23_001 = e001y, E23_101 = ecc(S, n, c101, 1);
-        T dzL14 = T(2) * (E22_000 - E23_000);
-        T dzR14 = T(2) * (E22_100 - E23_100);
-        T dzL34 = T(2) * (E23_001 - E22_000);
-        T dzR34 = T(2) * (E23_101 - E22_100);
-        T dz1214, dz1234;
-        upwind_pair(vx, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
-        T dxL14 = T(2) * (E21_000 - E23_000);
-        T dxR14 = T(2) * (E21_001 - E23_001);
-        T dxL34 = T(2) * (E23_100 - E21_000);
-        T dxR34 = T(2) * (E23_101 - E21_001);
-        T dx1412, dx3412;
-        upwind_pair(vz, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
-        E[(size_t)1 * n + c000] = T(0.25) * (E21_000 + E21_001 + E22_000 + E22_100) +
-                                  T(0.125) * ((dz1214 - dz1234) + (dx1412 - dx3412));
-    }
-    // Ex at (i, j+1/2, k+1/2)
-    {
-        T E11_000 = -Fy_bt1[c000], E11_001 = -Fy_bt1[c001];
-        T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
-        T E13_000 = e000x, E13_010 = e010x, E13_001 = e001x, E13_011 = ecc(S, n, c011, 0);
-        T dzL14 = T(2) * (E12_000 - E13_000);
-        T dzR14 = T(2) * (E12_010 - E13_010);
-        T dzL34 = T(2) * (E13_001 - E12_000);
-        T dzR34 = T(2) * (E13_011 - E12_010);
-        T dz1214, dz1234;
-        upwind_pair(vy, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
-        T dyL14 = T(2) * (E11_000 - E13_000);
-        T dyR14 = T(2) * (E11_001 - E13_001);
-        T dyL34 = T(2) * (E13_010 - E11_000);
-        T dyR34 = T(2) * (E13_011 - E11_001);
-        T dy1412, dy3412;
-        upwind_pair(vz, dyL14, dyR14, dyL34, dyR34, dy1412, dy3412);
-        E[c000] = T(0.25) * (E11_000 + E11_001 + E12_000 + E12_010) +
-                  T(0.125) * ((dz1214 - dz1234) + (dy1412 - dy3412));
+    CellEV<T> a000 = cell_ev(S, n, r000 + k0 * plane);
+    CellEV<T> a100 = cell_ev(S, n, r100 + k0 * plane);
+    CellEV<T> a010 = cell_ev(S, n, r010 + k0 * plane);
+    T fx2_000 = Fx_bt2[r000 + k0 * plane], fy1_000 = Fy_bt1[r000 + k0 * plane];
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k) {
+        const int kp = wrap_up(k, dm.nz);
+        const int c000 = r000 + k * plane, c100 = r100 + k * plane, c010 = r010 + k * plane;
+        const int c110 = r110 + k * plane;
+        const int c001 = r000 + kp * plane, c101 = r100 + kp * plane, c011 = r010 + kp * plane;
+        const CellEV<T> a001 = cell_ev(S, n, c001);
+        const CellEV<T> a101 = cell_ev(S, n, c101);
+        const CellEV<T> a011 = cell_ev(S, n, c011);
+        const T e110z = ecc(S, n, c110, 2);
+        const T fx2_001 = Fx_bt2[c001], fy1_001 = Fy_bt1[c001];
+        const T vx = T(0.5) * (a000.ux + a100.ux);
+        const T vy = T(0.5) * (a000.uy + a010.uy);
+        const T vz = T(0.5) * (a000.uz + a001.uz);
+        // Ez at (i+1/2, j+1/2, k)
+        {
+            T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
+            T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
+            T E33_000 = a000.ez, E33_100 = a100.ez, E33_010 = a010.ez, E33_110 = e110z;
+            T dyL14 = T(2) * (E32_000 - E33_000);
+            T dyR14 = T(2) * (E32_100 - E33_100);
+            T dyL34 = T(2) * (E33_010 - E32_000);
+            T dyR34 = T(2) * (E33_110 - E32_100);
+            T dy1214, dy1234;
+            upwind_pair(vx, dyL14, dyR14, dyL34, dyR34, dy1214, dy1234);
+            T dxL14 = T(2) * (E31_000 - E33_000);
+            T dxR14 = T(2) * (E31_010 - E33_010);
+            T dxL34 = T(2) * (E33_100 - E31_000);
+            T dxR34 = T(2) * (E33_110 - E31_010);
+            T dx1412, dx3412;
+            upwind_pair(vy, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+            E[(size_t)2 * n + c000] = T(0.25) * (E31_000 + E31_010 + E32_000 + E32_100) +
+                                      T(0.125) * ((dy1214 - dy1234) + (dx1412 - dx3412));
+        }
+        // Ey at (i+1/2, j, k+1/2)
+        {
+            T E21_000 = fx2_000, E21_001 = fx2_001;
+            T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
+            T E23_000 = a000.ey, E23_100 = a100.ey, E23_001 = a001.ey, E23_101 = a101.ey;
+            T dzL14 = T(2) * (E22_000 - E23_000);
+            T dzR14 = T(2) * (E22_100 - E23_100);
+            T dzL34 = T(2) * (E23_001 - E22_000);
+            T dzR34 = T(2) * (E23_101 - E22_100);
+            T dz1214, dz1234;
+            upwind_pair(vx, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+            T dxL14 = T(2) * (E21_000 - E23_000);
+            T dxR14 = T(2) * (E21_001 - E23_001);
+            T dxL34 = T(2) * (E23_100 - E21_000);
+            T dxR34 = T(2) * (E23_101 - E21_001);
+            T dx1412, dx3412;
+            upwind_pair(vz, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+            E[(size_t)1 * n + c000] = T(0.25) * (E21_000 + E21_001 + E22_000 + E22_100) +
+                                      T(0.125) * ((dz1214 - dz1234) + (dx1412 - dx3412));
+        }
+        // Ex at (i, j+1/2, k+1/2)
+        {
+            T E11_000 = -fy1_000, E11_001 = -fy1_001;
+            T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
+            T E13_000 = a000.ex, E13_010 = a010.ex, E13_001 = a001.ex, E13_011 = a011.ex;
+            T dzL14 = T(2) * (E12_000 - E13_000);
+            T dzR14 = T(2) * (E12_010 - E13_010);
+            T dzL34 = T(2) * (E13_001 - E12_000);
+            T dzR34 = T(2) * (E13_011 - E12_010);
+            T dz1214, dz1234;
+            upwind_pair(vy, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+            T dyL14 = T(2) * (E11_000 - E13_000);
+            T dyR14 = T(2) * (E11_001 - E13_001);
+            T dyL34 = T(2) * (E13_010 - E11_000);
+            T dyR34 = T(2) * (E13_011 - E11_001);
+            T dy1412, dy3412;
+            upwind_pair(vz, dyL14, dyR14, dyL34, dyR34, dy1412, dy3412);
+            E[c000] = T(0.25) * (E11_000 + E11_001 + E12_000 + E12_010) +
+                      T(0.125) * ((dz1214 - dz1234) + (dy1412 - dy3412));
+        }
+        a000 = a001;
+        a100 = a101;
+        a010 = a011;
+        fx2_000 = fx2_001;
+        fy1_000 = fy1_001;
     }
 }
 
@@ -544,10 +601,13 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
     return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
 }
 
+// A thread walks a column of kSegZ cells along z; the z-face fluxes, the
+// corner EMFs at k and the new face field bz read or computed at plane k are
+// the "k-1" values of plane k+1 and are carried instead of reloaded.
 template <class T, bool ONE>
-__global__ void __launch_bounds__(kBX) k_update(BatchArgs ba, double dt_scale, int final_stage) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArgs ba, double dt_scale, int final_stage) {
     int local;
-    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
@@ -561,54 +621,85 @@ __global__ void __launch_bounds__(kBX) k_update(BatchArgs ba, double dt_scale, i
     unsigned long long* cmax_slots = sc->cmax_slots;
     unsigned long long* floor_hits = &sc->floor_hits;
     unsigned int* status = &sc->status;
-    int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
-    bool valid = i < dm.nx;
+    int i, j, k0, k1;
+    decode_cellz<ONE>(local, dm, i, j, k0, k1);
+    const bool valid = i < dm.nx;
     double cmax = 0.0;
     if (valid) {
         const int n = dm.n;
-        T dtdx = (T)(dt_scale * sc->dt / dx);
-        int im = wrap_dn(i, dm.nx), jm = wrap_dn(j, dm.ny), km = wrap_dn(k, dm.nz);
-        auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
-        int c = C(i, j, k), cxm = C(im, j, k), cym = C(i, jm, k), czm = C(i, j, km);
-        T out[4];
+        const T dtdx = (T)(dt_scale * sc->dt / dx);
+        const int plane = dm.nx * dm.ny;
+        const int im = wrap_dn(i, dm.nx), jm = wrap_dn(j, dm.ny);
+        const int r0 = i + dm.nx * j, rxm = im + dm.nx * j, rym = i + dm.nx * jm, rxmym = im + dm.nx * jm;
+        const T* Ex = E;
+        const T* Ey = E + (size_t)n;
+        // values of plane k-1 (periodic image for the first cell of the column)
+        T Fzm[4], Ex_zm, Ey_zm, Ex_ymzm, Ey_xmzm, bzm;
+        {
+            const int km = wrap_dn(k0, dm.nz);
+            const int czm = r0 + km * plane, cxmzm = rxm + km * plane, cymzm = rym + km * plane;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            // flux component of xyz variable v in sweep D: rho -> 0; momentum X -> 1 + (X - D) mod 3
-            int fx = (v == 0) ? 0 : 1 + (v - 1 + 3) % 3;
-            int fy = (v == 0) ? 0 : 1 + (v - 1 - 1 + 3) % 3;
-            int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
-            const T* Fx = F + (size_t)(0 + fx) * n;
-            const T* Fy = F + (size_t)(6 + fy) * n;
-            const T* Fz = F + (size_t)(12 + fz) * n;
-            out[v] = fld(S0, v, n)[c] - dtdx * ((Fx[c] - Fx[cxm]) + (Fy[c] - Fy[cym]) + (Fz[c] - Fz[czm]));
+            for (int v = 0; v < 4; ++v) {
+                int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
+                Fzm[v] = F[(size_t)(12 + fz) * n + czm];
+            }
+            Ex_zm = Ex[czm];
+            Ey_zm = Ey[czm];
+            Ex_ymzm = Ex[cymzm];
+            Ey_xmzm = Ey[cxmzm];
+            bzm = ct_bz(S0, E, n, dtdx, czm, cxmzm, cymzm);
         }
-        if (out[0] < T(kMIN_DENS)) {
-            out[0] = T(kMIN_DENS);
-            atomicAdd(floor_hits, 1ull);
-        }
-        int cxmym = C(im, jm, k), cxmzm = C(im, j, km), cymzm = C(i, jm, km);
-        T bx = ct_bx(S0, E, n, dtdx, c, cym, czm);
-        T by = ct_by(S0, E, n, dtdx, c, czm, cxm);
-        T bz = ct_bz(S0, E, n, dtdx, c, cxm, cym);
-        T bxm = ct_bx(S0, E, n, dtdx, cxm, cxmym, cxmzm);
-        T bym = ct_by(S0, E, n, dtdx, cym, cymzm, cxmym);
-        T bzm = ct_bz(S0, E, n, dtdx, czm, cxmzm, cymzm);
-        T bxc = T(0.5) * (bx + bxm);
-        T byc = T(0.5) * (by + bym);
-        T bzc = T(0.5) * (bz + bzm);
+#pragma unroll 2
+        for (int k = k0; k < k1; ++k) {
+            const int c = r0 + k * plane, cxm = rxm + k * plane, cym = rym + k * plane, cxmym = rxmym + k * plane;
+            T out[4], Fz0[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
-        fld(Sout, 4, n)[c] = bxc;
-        fld(Sout, 5, n)[c] = byc;
-        fld(Sout, 6, n)[c] = bzc;
-        fld(Sout, 7, n)[c] = bx;
-        fld(Sout, 8, n)[c] = by;
-        fld(Sout, 9, n)[c] = bz;
-        if (do_cfl) cmax = (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr);
-        if (!(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
-              isfinite(by) && isfinite(bz)))
-            atomicOr(status, 2u);
+            for (int v = 0; v < 4; ++v) {
+                // flux component of xyz variable v in sweep D: rho -> 0; momentum X -> 1 + (X - D) mod 3
+                int fx = (v == 0) ? 0 : 1 + (v - 1 + 3) % 3;
+                int fy = (v == 0) ? 0 : 1 + (v - 1 - 1 + 3) % 3;
+                int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
+                const T* Fx = F + (size_t)(0 + fx) * n;
+                const T* Fy = F + (size_t)(6 + fy) * n;
+                Fz0[v] = F[(size_t)(12 + fz) * n + c];
+                out[v] = fld(S0, v, n)[c] - dtdx * ((Fx[c] - Fx[cxm]) + (Fy[c] - Fy[cym]) + (Fz0[v] - Fzm[v]));
+            }
+            if (out[0] < T(kMIN_DENS)) {
+                out[0] = T(kMIN_DENS);
+                atomicAdd(floor_hits, 1ull);
+            }
+            const T Ex0 = Ex[c], Ey0 = Ey[c], Ez0 = E[2 * (size_t)n + c];
+            const T Ex_ym = Ex[cym], Ey_xm = Ey[cxm];
+            const T Ez_ym = E[2 * (size_t)n + cym], Ez_xm = E[2 * (size_t)n + cxm], Ez_xmym = E[2 * (size_t)n + cxmym];
+            // ct_bx / ct_by / ct_bz of the face fields at c and at the minus faces
+            const T bx = fld(S0, 7, n)[c] - dtdx * ((Ez0 - Ez_ym) - (Ey0 - Ey_zm));
+            const T by = fld(S0, 8, n)[c] - dtdx * ((Ex0 - Ex_zm) - (Ez0 - Ez_xm));
+            const T bz = fld(S0, 9, n)[c] - dtdx * ((Ey0 - Ey_xm) - (Ex0 - Ex_ym));
+            const T bxm = fld(S0, 7, n)[cxm] - dtdx * ((Ez_xm - Ez_xmym) - (Ey_xm - Ey_xmzm));
+            const T bym = fld(S0, 8, n)[cym] - dtdx * ((Ex_ym - Ex_ymzm) - (Ez_ym - Ez_xmym));
+            const T bxc = T(0.5) * (bx + bxm);
+            const T byc = T(0.5) * (by + bym);
+            const T bzc = T(0.5) * (bz + bzm);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
+            fld(Sout, 4, n)[c] = bxc;
+            fld(Sout, 5, n)[c] = byc;
+            fld(Sout, 6, n)[c] = bzc;
+            fld(Sout, 7, n)[c] = bx;
+            fld(Sout, 8, n)[c] = by;
+            fld(Sout, 9, n)[c] = bz;
+            if (do_cfl) cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
+            if (!(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
+                  isfinite(by) && isfinite(bz)))
+                atomicOr(status, 2u);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Fzm[v] = Fz0[v];
+            Ex_zm = Ex0;
+            Ey_zm = Ey0;
+            Ex_ymzm = Ex_ym;
+            Ey_xmzm = Ey_xm;
+            bzm = bz;
+        }
     }
     if (do_cfl) block_atomic_max<kBX>(cmax_slots, cmax);
 }
@@ -629,10 +720,12 @@ __device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int c
 // Predictor: s_h = s - (dt/2dx) sum_d v_d (F_d(i+1/2) - F_d(i-1/2)) with
 // first-order upwind fluxes and the step-start velocity (passive_mod.f90:
 // 133-157, 204-224, 562-590).
-template <class T, bool ONE>
+// A thread walks a column of kSegZ cells along z, carrying the z-neighbour
+// velocities and scalars of the previous cell.
+template <class T, bool ONE, int NP>
 __global__ void __launch_bounds__(kBX) k_passive_pred(BatchArgs ba) {
     int local;
-    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     const Scalars* sc = rp.sc;
     const int npass = rp.npass;
     if (!rp.active || npass == 0) return;
@@ -640,33 +733,47 @@ __global__ void __launch_bounds__(kBX) k_passive_pred(BatchArgs ba) {
     const T* __restrict__ S0 = (const T*)rp.S[0];
     T* __restrict__ SH = (T*)rp.SH;
     const double dx = rp.dx;
-    int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
+    int i, j, k0, k1;
+    decode_cellz<ONE>(local, dm, i, j, k0, k1);
     if (i >= dm.nx) return;
     const int n = dm.n;
-    T dtdx = (T)(0.5 * sc->dt / dx);
-    auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
-    int c = C(i, j, k);
-    int cm[3] = {C(wrap_dn(i, dm.nx), j, k), C(i, wrap_dn(j, dm.ny), k), C(i, j, wrap_dn(k, dm.nz))};
-    int cp[3] = {C(wrap_up(i, dm.nx), j, k), C(i, wrap_up(j, dm.ny), k), C(i, j, wrap_up(k, dm.nz))};
-    T v0[3], vm[3], vp[3];
+    const int plane = dm.nx * dm.ny;
+    const T dtdx = (T)(0.5 * sc->dt / dx);
+    const int r0 = i + dm.nx * j;
+    const int rxm = wrap_dn(i, dm.nx) + dm.nx * j, rxp = wrap_up(i, dm.nx) + dm.nx * j;
+    const int rym = i + dm.nx * wrap_dn(j, dm.ny), ryp = i + dm.nx * wrap_up(j, dm.ny);
+    // z neighbours of the first cell
+    const int ckm = r0 + wrap_dn(k0, dm.nz) * plane, ck0 = r0 + k0 * plane;
+    T vz_m = vel_of(S0, n, ckm, 2), vz_0 = vel_of(S0, n, ck0, 2);
+    T s_m[NP], s_0[NP];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        v0[d] = vel_of(S0, n, c, d);
-        vm[d] = vel_of(S0, n, cm[d], d);
-        vp[d] = vel_of(S0, n, cp[d], d);
-    }
-    for (int p = 0; p < npass; ++p) {
-        const T* s = fld(S0, 10 + p, n);
-        T s0 = s[c];
-        T dF[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            T Fp = upwind_flux(s0, s[cp[d]], T(0.5) * (v0[d] + vp[d]));
-            T Fm = upwind_flux(s[cm[d]], s0, T(0.5) * (vm[d] + v0[d]));
-            dF[d] = Fp - Fm;
+    for (int p = 0; p < NP; ++p)
+        if (p < npass) {
+            s_m[p] = fld(S0, 10 + p, n)[ckm];
+            s_0[p] = fld(S0, 10 + p, n)[ck0];
         }
-        fld(SH, p, n)[c] = s0 - dtdx * (v0[0] * dF[0] + v0[1] * dF[1] + v0[2] * dF[2]);
+    for (int k = k0; k < k1; ++k) {
+        const int c = r0 + k * plane, czp = r0 + wrap_up(k, dm.nz) * plane;
+        const int cxm = rxm + k * plane, cxp = rxp + k * plane, cym = rym + k * plane, cyp = ryp + k * plane;
+        const T vx0 = vel_of(S0, n, c, 0), vy0 = vel_of(S0, n, c, 1);
+        const T vxm = vel_of(S0, n, cxm, 0), vxp = vel_of(S0, n, cxp, 0);
+        const T vym = vel_of(S0, n, cym, 1), vyp = vel_of(S0, n, cyp, 1);
+        const T vz_p = vel_of(S0, n, czp, 2);
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            if (p >= npass) break;
+            const T* s = fld(S0, 10 + p, n);
+            const T s0 = s_0[p], s_zp = s[czp];
+            T dF[3];
+            dF[0] = upwind_flux(s0, s[cxp], T(0.5) * (vx0 + vxp)) - upwind_flux(s[cxm], s0, T(0.5) * (vxm + vx0));
+            dF[1] = upwind_flux(s0, s[cyp], T(0.5) * (vy0 + vyp)) - upwind_flux(s[cym], s0, T(0.5) * (vym + vy0));
+            dF[2] = upwind_flux(s0, s_zp, T(0.5) * (vz_0 + vz_p)) - upwind_flux(s_m[p], s0, T(0.5) * (vz_m + vz_0));
+            fld(SH, p, n)[c] = s0 - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
+            s_m[p] = s0;
+            s_0[p] = s_zp;
+        }
+        vz_m = vz_0;
+        vz_0 = vz_p;
     }
 }
 
@@ -692,10 +799,12 @@ __device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict
     return T(0.5) * (vold + m1 * irho);
 }
 
-template <class T, bool ONE>
+// A thread walks a column of kSegZ cells along z, carrying the z-neighbour
+// time-averaged velocities, half-step scalars and their minmod slopes.
+template <class T, bool ONE, int NP>
 __global__ void __launch_bounds__(kBX) k_passive_corr(BatchArgs ba) {
     int local;
-    const BoxRec rp = resolve<ONE>(ba, kKindCell, local);
+    const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     const Scalars* sc = rp.sc;
     const int npass = rp.npass;
     if (!rp.active || npass == 0) return;
@@ -707,57 +816,95 @@ __global__ void __launch_bounds__(kBX) k_passive_corr(BatchArgs ba) {
     const int drive = sc->drive;
     const T* __restrict__ mbnd = (const T*)rp.mbnd;
     const int plane_stride = rp.plane_stride;
-    int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
+    int i, j, k0, k1;
+    decode_cellz<ONE>(local, dm, i, j, k0, k1);
     if (i >= dm.nx) return;
     const int n = dm.n;
-    T dtdx = (T)(sc->dt / dx);
-    auto C = [&](int a, int b, int cc) { return a + dm.nx * (b + dm.ny * cc); };
-    int idx[3] = {i, j, k};
-    int nn[3] = {dm.nx, dm.ny, dm.nz};
-    int c = C(i, j, k);
-    int cm[3], cp[3], cm2[3], cp2[3];
+    const int plane = dm.nx * dm.ny;
+    const T dtdx = (T)(sc->dt / dx);
+    const int r0 = i + dm.nx * j;
+    const int rxm = wrap_dn(i, dm.nx) + dm.nx * j, rxp = wrap_up(i, dm.nx) + dm.nx * j;
+    const int rxm2 = wrap_any(i - 2, dm.nx) + dm.nx * j, rxp2 = wrap_any(i + 2, dm.nx) + dm.nx * j;
+    const int rym = i + dm.nx * wrap_dn(j, dm.ny), ryp = i + dm.nx * wrap_up(j, dm.ny);
+    const int rym2 = i + dm.nx * wrap_any(j - 2, dm.ny), ryp2 = i + dm.nx * wrap_any(j + 2, dm.ny);
+    // on drive steps the velocity across the global boundary of axis d uses
+    // the unforced momentum of the ghost image (mbnd planes, see k_force_kick)
+    const T* um_x = (drive && i == 0) ? mbnd + (size_t)1 * plane_stride : nullptr;            // plane i = n-1
+    const T* up_x = (drive && i == dm.nx - 1) ? mbnd + (size_t)0 * plane_stride : nullptr;    // plane i = 0
+    const T* um_y = (drive && j == 0) ? mbnd + (size_t)3 * plane_stride : nullptr;
+    const T* up_y = (drive && j == dm.ny - 1) ? mbnd + (size_t)2 * plane_stride : nullptr;
+    const T* um_z = drive ? mbnd + (size_t)5 * plane_stride + (i + dm.nx * j) : nullptr;
+    const T* up_z = drive ? mbnd + (size_t)4 * plane_stride + (i + dm.nx * j) : nullptr;
+    // z neighbours of the first cell: velocities at k-1, k; scalars at
+    // k-2..k+1 and the minmod slopes at k-1, k
+    const int km = wrap_dn(k0, dm.nz);
+    const int ckm = r0 + km * plane, ck0 = r0 + k0 * plane;
+    T vz_m = vtavg(S0, S1, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
+    T vz_0 = vtavg(S0, S1, n, ck0, 2, (const T*)nullptr);
+    T s_m[NP], s_0[NP], s_p[NP], dl_m[NP], dl_0[NP];
+    {
+        const int ckm2 = r0 + wrap_any(k0 - 2, dm.nz) * plane, ckp = r0 + wrap_up(k0, dm.nz) * plane;
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        int t[3] = {i, j, k};
-        t[d] = wrap_dn(idx[d], nn[d]); cm[d] = C(t[0], t[1], t[2]);
-        t[d] = wrap_any(idx[d] - 2, nn[d]); cm2[d] = C(t[0], t[1], t[2]);
-        t[d] = wrap_up(idx[d], nn[d]); cp[d] = C(t[0], t[1], t[2]);
-        t[d] = wrap_any(idx[d] + 2, nn[d]); cp2[d] = C(t[0], t[1], t[2]);
+        for (int p = 0; p < NP; ++p)
+            if (p < npass) {
+                const T* s = fld(SH, p, n);
+                const T sm2 = s[ckm2];
+                s_m[p] = s[ckm];
+                s_0[p] = s[ck0];
+                s_p[p] = s[ckp];
+                dl_m[p] = minmod(sm2, s_m[p], s_0[p]);
+                dl_0[p] = minmod(s_m[p], s_0[p], s_p[p]);
+            }
     }
-    T vt0[3], vtm[3], vtp[3];
+    for (int k = k0; k < k1; ++k) {
+        const int kp = wrap_up(k, dm.nz);
+        const int c = r0 + k * plane, czp = r0 + kp * plane, czp2 = r0 + wrap_any(k + 2, dm.nz) * plane;
+        const int cxm = rxm + k * plane, cxp = rxp + k * plane, cxm2 = rxm2 + k * plane, cxp2 = rxp2 + k * plane;
+        const int cym = rym + k * plane, cyp = ryp + k * plane, cym2 = rym2 + k * plane, cyp2 = ryp2 + k * plane;
+        const int pofs_x = j + dm.ny * k, pofs_y = i + dm.nx * k;
+        const T vx0 = vtavg(S0, S1, n, c, 0, (const T*)nullptr);
+        const T vy0 = vtavg(S0, S1, n, c, 1, (const T*)nullptr);
+        const T vxm = vtavg(S0, S1, n, cxm, 0, um_x ? um_x + pofs_x : (const T*)nullptr);
+        const T vxp = vtavg(S0, S1, n, cxp, 0, up_x ? up_x + pofs_x : (const T*)nullptr);
+        const T vym = vtavg(S0, S1, n, cym, 1, um_y ? um_y + pofs_y : (const T*)nullptr);
+        const T vyp = vtavg(S0, S1, n, cyp, 1, up_y ? up_y + pofs_y : (const T*)nullptr);
+        const T vz_p = vtavg(S0, S1, n, czp, 2, (k == dm.nz - 1) ? up_z : (const T*)nullptr);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        vt0[d] = vtavg(S0, S1, n, c, d, (const T*)nullptr);
-        const T* um = nullptr;
-        const T* up = nullptr;
-        if (drive) {
-            // transverse position of the cell inside the boundary plane of axis d
-            int a = (d == 0) ? j : i;
-            int b = (d == 2) ? j : k;
-            int pn = (d == 0) ? dm.ny : dm.nx;
-            int pofs = a + pn * b;
-            if (idx[d] == 0) um = mbnd + (size_t)(2 * d + 1) * plane_stride + pofs;            // ghost = plane n-1
-            if (idx[d] == nn[d] - 1) up = mbnd + (size_t)(2 * d + 0) * plane_stride + pofs;    // ghost = plane 0
+        for (int p = 0; p < NP; ++p) {
+            if (p >= npass) break;
+            const T* s = fld(SH, p, n);
+            const T s0 = s_0[p];
+            T dF[3];
+            {
+                const T sm = s[cxm], sp = s[cxp], sm2 = s[cxm2], sp2 = s[cxp2];
+                const T dlm = minmod(sm2, sm, s0), dl0 = minmod(sm, s0, sp), dlp = minmod(s0, sp, sp2);
+                const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vx0 + vxp));
+                const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vxm + vx0));
+                dF[0] = Fp - Fm;
+            }
+            {
+                const T sm = s[cym], sp = s[cyp], sm2 = s[cym2], sp2 = s[cyp2];
+                const T dlm = minmod(sm2, sm, s0), dl0 = minmod(sm, s0, sp), dlp = minmod(s0, sp, sp2);
+                const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vy0 + vyp));
+                const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vym + vy0));
+                dF[1] = Fp - Fm;
+            }
+            {
+                const T sm = s_m[p], sp = s_p[p], sp2 = s[czp2];
+                const T dlm = dl_m[p], dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
+                const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vz_0 + vz_p));
+                const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vz_m + vz_0));
+                dF[2] = Fp - Fm;
+                s_m[p] = s0;
+                s_0[p] = sp;
+                s_p[p] = sp2;
+                dl_m[p] = dl0;
+                dl_0[p] = dlp;
+            }
+            fld(S1, 10 + p, n)[c] = fld(S0, 10 + p, n)[c] - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
         }
-        vtm[d] = vtavg(S0, S1, n, cm[d], d, um);
-        vtp[d] = vtavg(S0, S1, n, cp[d], d, up);
-    }
-    for (int p = 0; p < npass; ++p) {
-        const T* s = fld(SH, p, n);
-        T s0 = s[c];
-        T dF[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            T sm = s[cm[d]], sp = s[cp[d]], sm2 = s[cm2[d]], sp2 = s[cp2[d]];
-            T dlm = minmod(sm2, sm, s0);
-            T dl0 = minmod(sm, s0, sp);
-            T dlp = minmod(s0, sp, sp2);
-            T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vt0[d] + vtp[d]));
-            T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vtm[d] + vt0[d]));
-            dF[d] = Fp - Fm;
-        }
-        fld(S1, 10 + p, n)[c] = fld(S0, 10 + p, n)[c] - dtdx * (vt0[0] * dF[0] + vt0[1] * dF[1] + vt0[2] * dF[2]);
+        vz_m = vz_0;
+        vz_0 = vz_p;
     }
 }
 

@@ -33,6 +33,7 @@ static dim3 grid_of(const BatchDev& b, int kind) {
         const BoxRec& r = b.a.one;
         unsigned nbx = (unsigned)((r.nx + kBX - 1) / kBX);
         if (kind == kKindCell) return dim3(nbx, r.ny, r.nz);
+        if (kind == kKindCellZ) return dim3(nbx, r.ny, (unsigned)((r.nz + kSegZ - 1) / kSegZ));
         if (kind == kKindRed) return dim3((unsigned)r.nred);
         switch ((kind - kKindSolver0) % 5) {
             case kSubCell: return dim3(nbx, r.ny, r.nz);
@@ -104,6 +105,7 @@ static void launch_fluxes_corr_march(BatchDev& b) {
 template <class T, bool ONE>
 static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     const dim3 gc = grid_of<ONE>(b, kKindCell);
+    const dim3 gz = grid_of<ONE>(b, kKindCellZ);
     const int nfin = (b.a.nbox + 31) / 32;
     b.prof_mask = 0;
     if (device_driven) {
@@ -122,9 +124,9 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     if (b.has_solver[2]) launch_fluxes_pred<T, 2, ONE>(b);
     if (b.has_solver[3]) launch_fluxes_pred<T, 3, ONE>(b);
     mark(b, kStPredEmf);
-    k_corner_emf<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 0);
+    k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
     mark(b, kStPredUpdate);
-    k_update<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 0.5, 0);
+    k_update<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
     b.launches += 2;
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
@@ -141,9 +143,9 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     if (b.has_solver[2]) launch_fluxes_corr_march<T, 2, 2, ONE>(b);
     if (b.has_solver[3]) launch_fluxes_corr_march<T, 3, 2, ONE>(b);
     mark(b, kStCorrEmf);
-    k_corner_emf<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 1);
+    k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
     mark(b, kStFinalUpdate);
-    k_update<T, ONE><<<gc, kBX, 0, b.st>>>(b.a, 1.0, 1);
+    k_update<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
     b.launches += 2;
     if (b.drive_mode) {
         mark(b, kStForceKick);
@@ -152,9 +154,20 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     }
     if (b.any_pass) {
         mark(b, kStPassivePred);
-        k_passive_pred<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);
-        mark(b, kStPassiveCorr);
-        k_passive_corr<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);
+        // scalar arrays sized for the table's largest passive count
+        if (b.npass_max <= 2) {
+            k_passive_pred<T, ONE, 2><<<gz, kBX, 0, b.st>>>(b.a);
+            mark(b, kStPassiveCorr);
+            k_passive_corr<T, ONE, 2><<<gz, kBX, 0, b.st>>>(b.a);
+        } else if (b.npass_max <= 4) {
+            k_passive_pred<T, ONE, 4><<<gz, kBX, 0, b.st>>>(b.a);
+            mark(b, kStPassiveCorr);
+            k_passive_corr<T, ONE, 4><<<gz, kBX, 0, b.st>>>(b.a);
+        } else {
+            k_passive_pred<T, ONE, kMaxPass><<<gz, kBX, 0, b.st>>>(b.a);
+            mark(b, kStPassiveCorr);
+            k_passive_corr<T, ONE, kMaxPass><<<gz, kBX, 0, b.st>>>(b.a);
+        }
         b.launches += 2;
     }
     mark(b, kStFinalize);

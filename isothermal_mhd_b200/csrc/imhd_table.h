@@ -25,6 +25,7 @@ inline int reduction_blocks(int n) {
 inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
     long nbx = ceil_div(r.nx, kBX);
     if (kind == kKindCell) return nbx * r.ny * r.nz;
+    if (kind == kKindCellZ) return nbx * r.ny * ceil_div(r.nz, kSegZ);
     if (kind == kKindRed) return r.nred;
     int solver = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
@@ -73,9 +74,11 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
     bd.row_nx_max = 0;
     for (int s = 0; s < 4; ++s) bd.has_solver[s] = false;
     bd.any_pass = false;
+    bd.npass_max = 0;
     for (const BoxRec& r : recs) {
         if (r.riemann >= 1 && r.riemann <= 3) bd.has_solver[r.riemann] = true;
         if (r.npass > 0) bd.any_pass = true;
+        if (r.npass > bd.npass_max) bd.npass_max = r.npass;
         if (row_capable(r.nx, esz) && r.nx > bd.row_nx_max) bd.row_nx_max = r.nx;
     }
     bd.a.nbox = nbox;

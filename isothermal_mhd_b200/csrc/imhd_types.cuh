@@ -13,6 +13,7 @@ constexpr int kSlots = 64;     // spread of the max reductions over addresses
 constexpr int kBX = 128;       // threads along x of the per-cell kernels
 constexpr int kTX = 128;       // faces per block of the tiled x sweep
 constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
+constexpr int kSegZ = 16;      // cells per thread of the z-marching cell kernels
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocksMax = 1024;
 constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
@@ -29,7 +30,8 @@ enum Kind {
     kKindCell = 0,     // ceil(nx/kBX) * ny * nz blocks of kBX threads, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
     kKindSolver0 = 2,  // + 5*(solver-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another solver
-    kKinds = 17
+    kKindCellZ = 17,   // ceil(nx/kBX) * ny * ceil(nz/kSegZ) blocks of kBX threads, a z column of kSegZ cells per thread
+    kKinds = 18
 };
 __host__ __device__ constexpr int solver_kind(int solver, int sub) { return kKindSolver0 + 5 * (solver - 1) + sub; }
 enum SolverSub { kSubCell = 0, kSubXRow = 1, kSubXTile = 2, kSubMarchY = 3, kSubMarchZ = 4 };
@@ -99,6 +101,7 @@ struct BatchDev {
     int row_nx_max = 0;        // largest nx among boxes using the x-row sweep
     bool has_solver[4] = {false, false, false, false};
     bool any_pass = false;
+    int npass_max = 0;         // largest passive count of the table
     int drive_mode = 0;        // 0: no forcing, 1: every box drives (host decided), 2: per-box device flags
     int precision = 64;
     cudaStream_t st = nullptr;
