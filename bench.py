@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--riemann", default="roe")
+    ap.add_argument("--recon", default="plm", choices=["plm", "ppm"])
     ap.add_argument("--precision", type=int, default=32)
     ap.add_argument("--npass", type=int, default=2)
     ap.add_argument("--mach", type=float, default=2.0)
@@ -175,7 +176,7 @@ def run_ours(a, ws, rank, local):
     dev = torch.device("cuda", local)
     n = a.n
     q, b, p, delv, f = make_initial_state(n, a.mach, a.npass, a.seed + rank)
-    box = Box(n, precision=a.precision, riemann=a.riemann, npass=a.npass, cour=a.cour, edot=a.edot,
+    box = Box(n, precision=a.precision, riemann=a.riemann, recon=a.recon, npass=a.npass, cour=a.cour, edot=a.edot,
               dt_turb=0.05, device=local)
     stream = torch.cuda.current_stream(dev)
     box.set_stream(stream.cuda_stream)
@@ -316,7 +317,7 @@ def run_ours(a, ws, rank, local):
         "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if a.precision == 32 else "f64", "data": "synthetic (seeded OU turbulence)",
         "config": {"workload": WORKLOAD, "n": n, "precision": a.precision, "riemann": a.riemann,
-                   "recon": "plm-char", "npass": a.npass, "mach": a.mach, "edot": a.edot, "cour": a.cour,
+                   "recon": a.recon + "-char", "npass": a.npass, "mach": a.mach, "edot": a.edot, "cour": a.cour,
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (state %.1f GB)" %
                    ((10 + a.npass) * cells * esz / 1e9), "drive_steps_timed": state["drives"] - drives0},
         "gpu_launches": launches,

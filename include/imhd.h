@@ -59,7 +59,7 @@ typedef struct imhd_config {
     int nx, ny, nz;        /* interior cells per axis (constants_mod.f90:9-11) */
     int precision;         /* 64: FP64 everywhere; 32: FP32 bulk, FP64 reductions */
     int riemann;           /* IMHD_ROE / IMHD_HLLD / IMHD_HLLE */
-    int recon;             /* IMHD_PLM (IMHD_PPM is reserved) */
+    int recon;             /* IMHD_PLM or IMHD_PPM */
     int npass;             /* passive scalars, 0..8 (constants_mod.f90:63) */
     double sound_speed;    /* isothermal sound speed (constants_mod.f90:35) */
     double cour;           /* COUR_def (constants_mod.f90:16) */

@@ -17,14 +17,14 @@ from .box import RIEMANN, _dptr
 
 
 def make_config(n, precision=32, riemann="roe", npass=0, sound_speed=1.0, cour=0.4, edot=0.0, dt_turb=0.05,
-                ng=0, ng_pass=None, device=0):
+                ng=0, ng_pass=None, device=0, recon="plm"):
     nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(n)
     c = ImhdConfig()
     lib().imhd_default_config(ctypes.byref(c))
     c.nx, c.ny, c.nz = int(nx), int(ny), int(nz)
     c.precision = int(precision)
     c.riemann = RIEMANN[riemann] if isinstance(riemann, str) else int(riemann)
-    c.recon = 0
+    c.recon = {"plm": 0, "ppm": 1}[recon] if isinstance(recon, str) else int(recon)
     c.npass = int(npass)
     c.sound_speed = float(sound_speed)
     c.cour = float(cour)

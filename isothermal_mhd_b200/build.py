@@ -55,6 +55,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
     os.makedirs(BUILD_DIR, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "imhd.h")]
     objs = []
+    jobs = []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD_DIR, unit.replace(".cu", ".o"))
@@ -65,7 +66,16 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
+            jobs.append(cmd)
+    if ptxas_verbose:
+        for cmd in jobs:   # one at a time, so that the resource reports do not interleave
             subprocess.check_call(cmd)
+    else:
+        # the translation units compile in parallel (the two precisions dominate)
+        procs = [subprocess.Popen(cmd) for cmd in jobs]
+        failed = [cmd for cmd, p in zip(jobs, procs) if p.wait() != 0]
+        if failed:
+            raise subprocess.CalledProcessError(1, failed[0])
     if force or _stale(LIB, objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs
         if verbose:

@@ -165,7 +165,7 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         if ((double)c.nx * c.ny * c.nz >= 2147483647.0) return bfail(IMHD_E_ARG, "box too large");
         if (c.precision != 32 && c.precision != 64) return bfail(IMHD_E_ARG, "precision must be 32 or 64");
         if (c.riemann < 1 || c.riemann > 3) return bfail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
-        if (c.recon != IMHD_PLM) return bfail(IMHD_E_ARG, "only IMHD_PLM reconstruction is implemented");
+        if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) return bfail(IMHD_E_ARG, "recon must be IMHD_PLM or IMHD_PPM");
         if (c.npass < 0 || c.npass > imhd::kMaxPass) return bfail(IMHD_E_ARG, "npass must be in 0..8");
         if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return bfail(IMHD_E_ARG, "sound_speed and cour must be positive");
     }
@@ -183,7 +183,7 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
     bool forcing = false;
     for (int i = 0; i < nbox; ++i) {
         const imhd_config& c = cfgs[i];
-        imhd::init_rec(x->rec[i], c.nx, c.ny, c.nz, c.npass, c.riemann, c.sound_speed, c.cour, c.edot, c.dt_turb);
+        imhd::init_rec(x->rec[i], c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
         total += imhd::box_bytes(x->rec[i], x->esz, true);
         if ((size_t)x->rec[i].n > maxn) maxn = x->rec[i].n;
         forcing = forcing || c.edot > 0.0;

@@ -231,7 +231,7 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     if (c.ny > 65535 || c.nz > 65535) return fail(IMHD_E_ARG, "ny and nz must be <= 65535");
     if (c.precision != 32 && c.precision != 64) return fail(IMHD_E_ARG, "precision must be 32 or 64");
     if (c.riemann < 1 || c.riemann > 3) return fail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
-    if (c.recon != IMHD_PLM) return fail(IMHD_E_ARG, "only IMHD_PLM reconstruction is implemented");
+    if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) return fail(IMHD_E_ARG, "recon must be IMHD_PLM or IMHD_PPM");
     if (c.npass < 0 || c.npass > imhd::kMaxPass) return fail(IMHD_E_ARG, "npass must be in 0..8");
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return fail(IMHD_E_ARG, "sound_speed and cour must be positive");
     if (c.ng < 0 || c.ng_pass < 0) return fail(IMHD_E_ARG, "ghost widths must be >= 0");
@@ -243,7 +243,7 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     imhd_box* x = new imhd_box();
     x->cfg = c;
     x->esz = c.precision == 64 ? 8 : 4;
-    imhd::init_rec(x->rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.sound_speed, c.cour, c.edot, c.dt_turb);
+    imhd::init_rec(x->rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
     imhd::BatchDev& b = x->b;
     b.precision = c.precision;
     size_t N = (size_t)x->rec.n;

@@ -159,11 +159,12 @@ template <int D> struct Rot {
 // First-order interface fluxes (compute_{x,y,z}fluxes_3d with
 // corrector_stage = .FALSE., vanleer_mod.f90:441-478): left/right states are
 // the cell values, the normal field the face value.
-template <class T, int SOLVER, int D, bool ONE>
+template <class T, int SCHEME, int D, bool ONE>
 __global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
     using R = Rot<D>;
+    constexpr int SOLVER = scheme_solver(SCHEME);
     int local;
-    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubCell), local);
+    const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubCell), local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
@@ -230,13 +231,16 @@ __device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int 
 }
 
 // Sweeps along y (D=1) and z (D=2): one thread per (x, transverse) column
-// marches along the sweep direction over a segment of faces, keeping the
+// marches along the sweep direction over a segment of faces.  PLM keeps the
 // primitive window w(a-1..a+2) and the slopes delw(a), delw(a+1) in
-// registers.  Loads stay coalesced along x.
-template <class T, int SOLVER, int D, bool ONE>
+// registers; PPM keeps w(a..a+3), the slopes delw(a), delw(a+1) and the right
+// edge of cell a.  Loads stay coalesced along x.
+template <class T, int SCHEME, int D, bool ONE>
 __global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
+    constexpr int SOLVER = scheme_solver(SCHEME);
+    constexpr bool PPM = scheme_recon(SCHEME) == 1;
     int local;
-    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, D == 1 ? kSubMarchY : kSubMarchZ), local);
+    const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, D == 1 ? kSubMarchY : kSubMarchZ), local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
@@ -264,41 +268,82 @@ __global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
     if (valid) {
         int stride = (D == 1) ? dm.nx : dm.nx * dm.ny;
         int base = (D == 1) ? i + dm.nx * dm.ny * o : i + dm.nx * o;
-        T wa[6], wb_[6], wc[6], wd[6];   // w(a-1), w(a), w(a+1), w(a+2)
-        T bnA, bnB, tmpbn;
-        T dA[6], dB[6];                  // delw(a), delw(a+1)
-        load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wa, tmpbn);
-        load_prim<T, D>(S, dm.n, base + a0 * stride, wb_, bnA);
-        load_prim<T, D>(S, dm.n, base + wrap_up(a0, na) * stride, wc, bnB);
-        char_slope(wa, wb_, wc, bnA, cs, asqr, dA);
-        for (int a = a0; a < a1; ++a) {
-            int ap1 = wrap_up(a, na);
-            int ap2 = wrap_up(ap1, na);
-            T bnC;
-            load_prim<T, D>(S, dm.n, base + ap2 * stride, wd, bnC);
-            char_slope(wb_, wc, wd, bnB, cs, asqr, dB);
-            T qL[7], qR[7], Fo[7];
-            plm_left_state(wb_, dA, bnA, qL);
-            plm_right_state(wc, dB, bnA, qR);
-            riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
-            store_flux(F, D, dm.n, base + a * stride, Fo);
+        if constexpr (!PPM) {
+            T wa[6], wb_[6], wc[6], wd[6];   // w(a-1), w(a), w(a+1), w(a+2)
+            T bnA, bnB, tmpbn;
+            T dA[6], dB[6];                  // delw(a), delw(a+1)
+            load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wa, tmpbn);
+            load_prim<T, D>(S, dm.n, base + a0 * stride, wb_, bnA);
+            load_prim<T, D>(S, dm.n, base + wrap_up(a0, na) * stride, wc, bnB);
+            char_slope<T>(wa, wb_, wc, wc, bnA, cs, asqr, dA);
+            for (int a = a0; a < a1; ++a) {
+                int ap1 = wrap_up(a, na);
+                int ap2 = wrap_up(ap1, na);
+                T bnC;
+                load_prim<T, D>(S, dm.n, base + ap2 * stride, wd, bnC);
+                char_slope<T>(wb_, wc, wd, wd, bnB, cs, asqr, dB);
+                T qL[7], qR[7], Fo[7];
+                plm_left_state(wb_, dA, bnA, qL);
+                plm_right_state(wc, dB, bnA, qR);
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+                store_flux(F, D, dm.n, base + a * stride, Fo);
 #pragma unroll
-            for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
-            bnA = bnB; bnB = bnC;
+                for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
+                bnA = bnB; bnB = bnC;
+            }
+        } else {
+            T w0[6], w1[6], w2[6], w3[6];    // w(a), w(a+1), w(a+2), w(a+3)
+            T bn0, bn1, bn2, bn3;
+            T d0[6], d1[6];                  // delw(a), delw(a+1)
+            T r0[6];                         // right edge of cell a
+            {
+                T wm2[6], wm1[6], dm1[6], l0[6], bnm2, bnm1;
+                load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 2, na) * stride, wm2, bnm2);
+                load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wm1, bnm1);
+                load_prim<T, D>(S, dm.n, base + a0 * stride, w0, bn0);
+                load_prim<T, D>(S, dm.n, base + wrap_any(a0 + 1, na) * stride, w1, bn1);
+                load_prim<T, D>(S, dm.n, base + wrap_any(a0 + 2, na) * stride, w2, bn2);
+                char_slope<T, true>(wm2, wm1, w0, w1, bnm1, cs, asqr, dm1);
+                char_slope<T, true>(wm1, w0, w1, w2, bn0, cs, asqr, d0);
+                ppm_edges(wm1, w0, w1, dm1, d0, l0, r0);
+            }
+            for (int a = a0; a < a1; ++a) {
+                load_prim<T, D>(S, dm.n, base + wrap_any(a + 3, na) * stride, w3, bn3);
+                char_slope<T, true>(w0, w1, w2, w3, bn1, cs, asqr, d1);
+                T l1[6], r1[6];
+                ppm_edges(w0, w1, w2, d0, d1, l1, r1);
+                T qL[7], qR[7], Fo[7];
+                ppm_state(r0, bn0, qL);
+                ppm_state(l1, bn0, qR);
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+                store_flux(F, D, dm.n, base + a * stride, Fo);
+#pragma unroll
+                for (int m = 0; m < 6; ++m) {
+                    w0[m] = w1[m]; w1[m] = w2[m]; w2[m] = w3[m];
+                    d0[m] = d1[m]; r0[m] = r1[m];
+                }
+                bn0 = bn1; bn1 = bn2; bn2 = bn3;
+            }
         }
     }
     block_atomic_max<kBX>(smax_slots, (double)smax);
 }
 
 // Sweep along x: a block covers TX faces of one (j,k) row; primitives of the
-// TX+3 cells and the TX+1 slopes are staged in shared memory.
-template <class T, int SOLVER, int TX, bool ONE>
+// TX+3 cells (PLM; TX+5 for PPM) and the TX+1 slopes (TX+2) are staged in
+// shared memory.
+template <class T, int SCHEME, int TX, bool ONE>
 __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
-    __shared__ T sw[6][TX + 3];
-    __shared__ T sbn[TX + 3];
-    __shared__ T sd[6][TX + 1];
+    constexpr int SOLVER = scheme_solver(SCHEME);
+    constexpr bool PPM = scheme_recon(SCHEME) == 1;
+    constexpr int H = PPM ? 2 : 1;           // cells staged left of the tile
+    constexpr int NW = TX + (PPM ? 5 : 3);   // staged cells
+    constexpr int ND = TX + (PPM ? 2 : 1);   // staged slopes, cells i0-H+1 ...
+    __shared__ T sw[6][NW];
+    __shared__ T sbn[NW];
+    __shared__ T sd[6][ND];
     int local;
-    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubXTile), local);
+    const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubXTile), local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
@@ -316,8 +361,9 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
         k = (local / nbt) / dm.ny;
     }
     int row = dm.nx * (j + dm.ny * k);
-    for (int t = threadIdx.x; t < TX + 3; t += TX) {
-        int ii = wrap_any(i0 - 1 + t, dm.nx);
+    // staged cell t is i0 - H + t
+    for (int t = threadIdx.x; t < NW; t += TX) {
+        int ii = wrap_any(i0 - H + t, dm.nx);
         T w[6], bn;
         load_prim<T, 0>(S, dm.n, row + ii, w, bn);
 #pragma unroll
@@ -325,26 +371,44 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
         sbn[t] = bn;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < TX + 1; t += TX) {
-        T wm[6], w0[6], wp[6], d[6];
+    // slope u is that of staged cell u + 1
+    for (int u = threadIdx.x; u < ND; u += TX) {
+        T wm[6], w0[6], wp[6], wp2[6], d[6];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) { wm[m] = sw[m][t]; w0[m] = sw[m][t + 1]; wp[m] = sw[m][t + 2]; }
-        char_slope(wm, w0, wp, sbn[t + 1], cs, asqr, d);
+        for (int m = 0; m < 6; ++m) {
+            wm[m] = sw[m][u]; w0[m] = sw[m][u + 1]; wp[m] = sw[m][u + 2];
+            wp2[m] = PPM ? sw[m][u + 3] : sw[m][u + 2];
+        }
+        char_slope<T, PPM>(wm, w0, wp, wp2, sbn[u + 1], cs, asqr, d);
 #pragma unroll
-        for (int m = 0; m < 6; ++m) sd[m][t] = d[m];
+        for (int m = 0; m < 6; ++m) sd[m][u] = d[m];
     }
     __syncthreads();
     int t = threadIdx.x;
     int i = i0 + t;
     T smax = T(0);
     if (i < dm.nx) {
-        T wl[6], wr[6], dl[6], dr[6];
-#pragma unroll
-        for (int m = 0; m < 6; ++m) { wl[m] = sw[m][t + 1]; wr[m] = sw[m][t + 2]; dl[m] = sd[m][t]; dr[m] = sd[m][t + 1]; }
-        T bn = sbn[t + 1];
+        // cell i is staged at t + H, its slope at t + H - 1
+        T bn = sbn[t + H];
         T qL[7], qR[7], Fo[7];
-        plm_left_state(wl, dl, bn, qL);
-        plm_right_state(wr, dr, bn, qR);
+        if constexpr (!PPM) {
+            T wl[6], wr[6], dl[6], dr[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) { wl[m] = sw[m][t + 1]; wr[m] = sw[m][t + 2]; dl[m] = sd[m][t]; dr[m] = sd[m][t + 1]; }
+            plm_left_state(wl, dl, bn, qL);
+            plm_right_state(wr, dr, bn, qR);
+        } else {
+            T wm[6], w0[6], wp[6], wp2[6], dm1[6], d0[6], dp[6], l[6], r[6], l1[6], r1[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                wm[m] = sw[m][t + 1]; w0[m] = sw[m][t + 2]; wp[m] = sw[m][t + 3]; wp2[m] = sw[m][t + 4];
+                dm1[m] = sd[m][t]; d0[m] = sd[m][t + 1]; dp[m] = sd[m][t + 2];
+            }
+            ppm_edges(wm, w0, wp, dm1, d0, l, r);      // cell i
+            ppm_edges(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
+            ppm_state(r, bn, qL);
+            ppm_state(l1, bn, qR);
+        }
         riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
@@ -354,13 +418,16 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
 // Sweep along x over whole rows: one block per (j,k) row.  The primitives,
 // face fields and slopes of the row live in shared memory and the periodic
 // wrap is an index wrap inside the row, so every cell's slope is computed
-// exactly once (the tiled kernel above recomputes one slope per tile and
-// stages a halo).  Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
-template <class T, int SOLVER, bool ONE>
+// exactly once (the tiled kernel above recomputes slopes at tile edges and
+// stages a halo).  PPM evaluates the edges of cells i and i+1 per face.
+// Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
+template <class T, int SCHEME, bool ONE>
 __global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
+    constexpr int SOLVER = scheme_solver(SCHEME);
+    constexpr bool PPM = scheme_recon(SCHEME) == 1;
     extern __shared__ __align__(16) unsigned char xrow_smem[];
     int local;
-    const BoxRec rp = resolve<ONE>(ba, solver_kind(SOLVER, kSubXRow), local);
+    const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubXRow), local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
     const Dims dm = dims_of(rp);
@@ -388,11 +455,14 @@ __global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
     }
     __syncthreads();
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        int im = wrap_dn(i, nx), ip = wrap_up(i, nx);
-        T wm[6], w0[6], wp[6], d[6];
+        int im = wrap_dn(i, nx), ip = wrap_up(i, nx), ip2 = wrap_up(ip, nx);
+        T wm[6], w0[6], wp[6], wp2[6], d[6];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) { wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip]; }
-        char_slope(wm, w0, wp, sbn[i], cs, asqr, d);
+        for (int m = 0; m < 6; ++m) {
+            wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip];
+            wp2[m] = PPM ? sw[m * nx + ip2] : wp[m];
+        }
+        char_slope<T, PPM>(wm, w0, wp, wp2, sbn[i], cs, asqr, d);
 #pragma unroll
         for (int m = 0; m < 6; ++m) sd[m * nx + i] = d[m];
     }
@@ -400,16 +470,30 @@ __global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
     T smax = T(0);
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         int ip = wrap_up(i, nx);
-        T wl[6], wr[6], dl[6], dr[6];
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            wl[m] = sw[m * nx + i]; wr[m] = sw[m * nx + ip];
-            dl[m] = sd[m * nx + i]; dr[m] = sd[m * nx + ip];
-        }
         T bn = sbn[i];
         T qL[7], qR[7], Fo[7];
-        plm_left_state(wl, dl, bn, qL);
-        plm_right_state(wr, dr, bn, qR);
+        if constexpr (!PPM) {
+            T wl[6], wr[6], dl[6], dr[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                wl[m] = sw[m * nx + i]; wr[m] = sw[m * nx + ip];
+                dl[m] = sd[m * nx + i]; dr[m] = sd[m * nx + ip];
+            }
+            plm_left_state(wl, dl, bn, qL);
+            plm_right_state(wr, dr, bn, qR);
+        } else {
+            int im = wrap_dn(i, nx), ip2 = wrap_up(ip, nx);
+            T wm[6], w0[6], wp[6], wp2[6], dm1[6], d0[6], dp[6], l[6], r[6], l1[6], r1[6];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip]; wp2[m] = sw[m * nx + ip2];
+                dm1[m] = sd[m * nx + im]; d0[m] = sd[m * nx + i]; dp[m] = sd[m * nx + ip];
+            }
+            ppm_edges(wm, w0, wp, dm1, d0, l, r);      // cell i
+            ppm_edges(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
+            ppm_state(r, bn, qL);
+            ppm_state(l1, bn, qR);
+        }
         riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
         store_flux(F, 0, dm.n, row + i, Fo);
     }

@@ -13,9 +13,22 @@
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+#include <utility>
+
 #include "imhd_kernels.cuh"
 
 namespace imhd {
+
+// Call f(std::integral_constant<int, s>) for every scheme s = 1..kSchemes.
+template <class Fn, int... S>
+inline void for_schemes_impl(Fn&& f, std::integer_sequence<int, S...>) {
+    (f(std::integral_constant<int, S + 1>{}), ...);
+}
+template <class Fn>
+inline void for_schemes(Fn&& f) {
+    for_schemes_impl(f, std::make_integer_sequence<int, kSchemes>{});
+}
 
 inline void mark(BatchDev& b, int stage) {
     if (!b.prof) return;
@@ -45,60 +58,64 @@ static dim3 grid_of(const BatchDev& b, int kind) {
     }
 }
 
-template <class T, int SOLVER, bool ONE>
+template <class T, int SCHEME, bool ONE>
 static void launch_fluxes_pred(BatchDev& b) {
-    if (b.totals[solver_kind(SOLVER, kSubCell)] == 0) return;
-    dim3 g = grid_of<ONE>(b, solver_kind(SOLVER, kSubCell));
-    k_pred_flux<T, SOLVER, 0, ONE><<<g, kBX, 0, b.st>>>(b.a);
-    k_pred_flux<T, SOLVER, 1, ONE><<<g, kBX, 0, b.st>>>(b.a);
-    k_pred_flux<T, SOLVER, 2, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    if (!b.has_scheme[SCHEME] || b.totals[scheme_kind(SCHEME, kSubCell)] == 0) return;
+    dim3 g = grid_of<ONE>(b, scheme_kind(SCHEME, kSubCell));
+    k_pred_flux<T, SCHEME, 0, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    k_pred_flux<T, SCHEME, 1, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    k_pred_flux<T, SCHEME, 2, ONE><<<g, kBX, 0, b.st>>>(b.a);
     b.launches += 3;
 }
 
 // The x-row sweep needs more than 48 KiB of dynamic shared memory for long
 // rows; the opt-in is per kernel and device and is done outside any capture.
-template <class T, int SOLVER, bool ONE>
+template <class T, int SCHEME, bool ONE>
 static void ensure_xrow_attr() {
     static bool attr_set[64] = {};   // per instantiation and device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        cudaFuncSetAttribute(k_corr_flux_xrow<T, SOLVER, ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRowSmemMax);
+        cudaFuncSetAttribute(k_corr_flux_xrow<T, SCHEME, ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRowSmemMax);
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
 }
 
 template <class T>
 cudaError_t prepare_launch(BatchDev& b) {
-    if (b.has_solver[1]) { ensure_xrow_attr<T, 1, true>(); ensure_xrow_attr<T, 1, false>(); }
-    if (b.has_solver[2]) { ensure_xrow_attr<T, 2, true>(); ensure_xrow_attr<T, 2, false>(); }
-    if (b.has_solver[3]) { ensure_xrow_attr<T, 3, true>(); ensure_xrow_attr<T, 3, false>(); }
+    for_schemes([&](auto s) {
+        if (b.has_scheme[s.value]) {
+            ensure_xrow_attr<T, s.value, true>();
+            ensure_xrow_attr<T, s.value, false>();
+        }
+    });
     return cudaGetLastError();
 }
 
-template <class T, int SOLVER, bool ONE>
+template <class T, int SCHEME, bool ONE>
 static void launch_fluxes_corr_x(BatchDev& b) {
-    if (b.totals[solver_kind(SOLVER, kSubXRow)]) {
-        dim3 gr = grid_of<ONE>(b, solver_kind(SOLVER, kSubXRow));
+    if (!b.has_scheme[SCHEME]) return;
+    if (b.totals[scheme_kind(SCHEME, kSubXRow)]) {
+        dim3 gr = grid_of<ONE>(b, scheme_kind(SCHEME, kSubXRow));
         size_t smem = 13 * (size_t)b.row_nx_max * sizeof(T);
-        ensure_xrow_attr<T, SOLVER, ONE>();
+        ensure_xrow_attr<T, SCHEME, ONE>();
         int bd = b.row_nx_max >= 256 ? 256 : ((b.row_nx_max + 31) / 32) * 32;
-        k_corr_flux_xrow<T, SOLVER, ONE><<<gr, bd, smem, b.st>>>(b.a);
+        k_corr_flux_xrow<T, SCHEME, ONE><<<gr, bd, smem, b.st>>>(b.a);
         b.launches += 1;
     }
-    if (b.totals[solver_kind(SOLVER, kSubXTile)]) {
-        dim3 gt = grid_of<ONE>(b, solver_kind(SOLVER, kSubXTile));
-        k_corr_flux_x<T, SOLVER, kTX, ONE><<<gt, kTX, 0, b.st>>>(b.a);
+    if (b.totals[scheme_kind(SCHEME, kSubXTile)]) {
+        dim3 gt = grid_of<ONE>(b, scheme_kind(SCHEME, kSubXTile));
+        k_corr_flux_x<T, SCHEME, kTX, ONE><<<gt, kTX, 0, b.st>>>(b.a);
         b.launches += 1;
     }
 }
 
-template <class T, int SOLVER, int D, bool ONE>
+template <class T, int SCHEME, int D, bool ONE>
 static void launch_fluxes_corr_march(BatchDev& b) {
-    const int kind = solver_kind(SOLVER, D == 1 ? kSubMarchY : kSubMarchZ);
-    if (b.totals[kind] == 0) return;
+    const int kind = scheme_kind(SCHEME, D == 1 ? kSubMarchY : kSubMarchZ);
+    if (!b.has_scheme[SCHEME] || b.totals[kind] == 0) return;
     dim3 g = grid_of<ONE>(b, kind);
-    k_corr_flux_march<T, SOLVER, D, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    k_corr_flux_march<T, SCHEME, D, ONE><<<g, kBX, 0, b.st>>>(b.a);
     b.launches += 1;
 }
 
@@ -120,9 +137,7 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     }
     // predictor: first-order fluxes, EMFs, half-dt update into the other buffer
     mark(b, kStPredFlux);
-    if (b.has_solver[1]) launch_fluxes_pred<T, 1, ONE>(b);
-    if (b.has_solver[2]) launch_fluxes_pred<T, 2, ONE>(b);
-    if (b.has_solver[3]) launch_fluxes_pred<T, 3, ONE>(b);
+    for_schemes([&](auto s) { launch_fluxes_pred<T, s.value, ONE>(b); });
     mark(b, kStPredEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
     mark(b, kStPredUpdate);
@@ -131,17 +146,11 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
     mark(b, kStCorrFluxX);
-    if (b.has_solver[1]) launch_fluxes_corr_x<T, 1, ONE>(b);
-    if (b.has_solver[2]) launch_fluxes_corr_x<T, 2, ONE>(b);
-    if (b.has_solver[3]) launch_fluxes_corr_x<T, 3, ONE>(b);
+    for_schemes([&](auto s) { launch_fluxes_corr_x<T, s.value, ONE>(b); });
     mark(b, kStCorrFluxY);
-    if (b.has_solver[1]) launch_fluxes_corr_march<T, 1, 1, ONE>(b);
-    if (b.has_solver[2]) launch_fluxes_corr_march<T, 2, 1, ONE>(b);
-    if (b.has_solver[3]) launch_fluxes_corr_march<T, 3, 1, ONE>(b);
+    for_schemes([&](auto s) { launch_fluxes_corr_march<T, s.value, 1, ONE>(b); });
     mark(b, kStCorrFluxZ);
-    if (b.has_solver[1]) launch_fluxes_corr_march<T, 1, 2, ONE>(b);
-    if (b.has_solver[2]) launch_fluxes_corr_march<T, 2, 2, ONE>(b);
-    if (b.has_solver[3]) launch_fluxes_corr_march<T, 3, 2, ONE>(b);
+    for_schemes([&](auto s) { launch_fluxes_corr_march<T, s.value, 2, ONE>(b); });
     mark(b, kStCorrEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
     mark(b, kStFinalUpdate);

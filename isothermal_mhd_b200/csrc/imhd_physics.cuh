@@ -415,8 +415,12 @@ __device__ __forceinline__ void prim_alphas_fp64(double rho, double bn, double w
     }
 }
 
-template <class T>
-__device__ __forceinline__ void plm_char_slope(const T* wm, const T* w0, const T* wp, T bn, T cs, T asqr, T* delw) {
+// With PPM the slope is the difference of the MC-limited characteristic
+// slopes of cells i+1 and i, both projected on the eigenvectors of cell i
+// (the PPM branch :1593-1627); wp2 is w(i+2) and is not read for PLM.
+template <class T, bool PPM = false>
+__device__ __forceinline__ void plm_char_slope(const T* wm, const T* w0, const T* wp, const T* wp2, T bn, T cs, T asqr,
+                                               T* delw) {
     const T ZERO = T(kZERO);
     T rho = w0[0];
     T irho = T(1) / rho;
@@ -491,10 +495,28 @@ __device__ __forceinline__ void plm_char_slope(const T* wm, const T* w0, const T
             aC = L[k][2] * w0[2] + L[k][3] * w0[3] + L[k][4] * w0[4] + L[k][5] * w0[5];
             aR = L[k][2] * wp[2] + L[k][3] * wp[3] + L[k][4] * wp[4] + L[k][5] * wp[5];
         }
-        T dL = aC - aL;
-        T dR = aR - aC;
-        T dC = T(0.5) * (dL + dR);
-        dm[k] = mc_limit(dL, dR, dC);
+        if constexpr (PPM) {
+            T aR2;
+            if (is_exact<T>::value || (k != 1 && k != 4))
+                aR2 = L[k][0] * wp2[0] + L[k][1] * wp2[1] + L[k][2] * wp2[2] + L[k][3] * wp2[3] + L[k][4] * wp2[4] +
+                      L[k][5] * wp2[5];
+            else
+                aR2 = L[k][2] * wp2[2] + L[k][3] * wp2[3] + L[k][4] * wp2[4] + L[k][5] * wp2[5];
+            T dL1 = aC - aL;
+            T dR1 = aR - aC;
+            T dC1 = T(0.5) * (dL1 + dR1);
+            T dL2 = aR - aC;
+            T dR2 = aR2 - aR;
+            T dC2 = T(0.5) * (dL2 + dR2);
+            T m1 = mc_limit(dL1, dR1, dC1);
+            T m2 = mc_limit(dL2, dR2, dC2);
+            dm[k] = m2 - m1;
+        } else {
+            T dL = aC - aL;
+            T dR = aR - aC;
+            T dC = T(0.5) * (dL + dR);
+            dm[k] = mc_limit(dL, dR, dC);
+        }
     }
     // right eigenvectors, columns (S08 A12): R(row r, column c)
     T R[6][6];
@@ -537,6 +559,51 @@ __device__ __forceinline__ void plm_right_state(const T* w, const T* d, T bn, T*
     q[4] = bn;
     q[5] = w[4] - T(0.5) * d[4];
     q[6] = w[5] - T(0.5) * d[5];
+    q[1] = q[1] * q[0];
+    q[2] = q[2] * q[0];
+    q[3] = q[3] * q[0];
+}
+
+// PPM edge values of cell i (vanleer_mod.f90:1660-1743): the parabola's
+// left and right values from the neighbour averages and the slope
+// differences delw(i-1) (dm) and delw(i) (d0), then the monotonicity
+// constraints (flatten at an extremum, steepen an overshooting edge).
+template <class T>
+__device__ __forceinline__ void ppm_edges(const T* wm, const T* w0, const T* wp, const T* dm, const T* d0, T* wl,
+                                          T* wr) {
+    const T sixth = T(1.0 / 6.0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        T l = T(0.5) * (wm[k] + w0[k]) - sixth * dm[k];
+        T r = T(0.5) * (w0[k] + wp[k]) - sixth * d0[k];
+        T c = w0[k];
+        T tmp1 = (r - c) * (c - l);
+        T tmp2 = T(6) * (r - l) * (c - T(0.5) * (l + r));
+        T tmp3 = sq(r - l);
+        if (tmp1 <= T(0)) {
+            l = c;
+            r = c;
+        } else if (tmp2 > tmp3) {
+            l = T(3) * c - T(2) * r;
+        } else if (tmp2 < -tmp3) {
+            r = T(3) * c - T(2) * l;
+        }
+        wl[k] = l;
+        wr[k] = r;
+    }
+}
+// Conserved interface state of face i+1/2 from a PPM edge (right edge of
+// cell i for the left state, left edge of cell i+1 for the right state) and
+// the face field (:1750-1778, 1799-1814).
+template <class T>
+__device__ __forceinline__ void ppm_state(const T* e, T bn, T* q) {
+    q[0] = e[0];
+    q[1] = e[1];
+    q[2] = e[2];
+    q[3] = e[3];
+    q[4] = bn;
+    q[5] = e[4];
+    q[6] = e[5];
     q[1] = q[1] * q[0];
     q[2] = q[2] * q[0];
     q[3] = q[3] * q[0];

@@ -282,8 +282,9 @@ __device__ __forceinline__ void flux_hlld_fast(const float* uL, const float* uR,
 // Limited characteristic slope of one cell (S08 A12/A22, vanleer_mod.f90:
 // 941-1141, 1507-1546), FP32.  wm, w0, wp: rotated primitives of cells
 // i-1, i, i+1; bn: face field at i+1/2.
-__device__ __forceinline__ void plm_char_slope_fast(const float* wm, const float* w0, const float* wp, float bn,
-                                                    float cs, float asqr, float* delw) {
+template <bool PPM = false>
+__device__ __forceinline__ void plm_char_slope_fast(const float* wm, const float* w0, const float* wp,
+                                                    const float* wp2, float bn, float cs, float asqr, float* delw) {
     float rho = w0[0];
     float irho = 1.0f / rho;
     float irhos = rsqrtf(rho);
@@ -324,14 +325,19 @@ __device__ __forceinline__ void plm_char_slope_fast(const float* wm, const float
     float hS = 0.5f * S * irhos;
     float dm[6];
     {
-        float dL[6], dR[6];
+        constexpr int NS = PPM ? 3 : 2;   // projected differences: w0-wm, wp-w0 (, wp2-wp)
+        float dD[NS][6];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) { dL[m] = w0[m] - wm[m]; dR[m] = wp[m] - w0[m]; }
-        float aL[6], aR[6];
+        for (int m = 0; m < 6; ++m) {
+            dD[0][m] = w0[m] - wm[m];
+            dD[1][m] = wp[m] - w0[m];
+            if constexpr (PPM) dD[2][m] = wp2[m] - wp[m];
+        }
+        float aD[NS][6];
 #pragma unroll
-        for (int s = 0; s < 2; ++s) {
-            const float* d = s ? dR : dL;
-            float* a = s ? aR : aL;
+        for (int s = 0; s < NS; ++s) {
+            const float* d = dD[s];
+            float* a = aD[s];
             float dvt = gy * d[2] + gz * d[3];
             float dbt = gy * d[4] + gz * d[5];
             float P = f0 * d[0] + fa * dbt, Q = fq * dvt - f1 * d[1];
@@ -342,7 +348,11 @@ __device__ __forceinline__ void plm_char_slope_fast(const float* wm, const float
             a[1] = U + V; a[4] = V - U;
         }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) dm[k] = mc_limit(aL[k], aR[k], 0.5f * (aL[k] + aR[k]));
+        for (int k = 0; k < 6; ++k) {
+            float m1 = mc_limit(aD[0][k], aD[1][k], 0.5f * (aD[0][k] + aD[1][k]));
+            if constexpr (PPM) dm[k] = mc_limit(aD[1][k], aD[2][k], 0.5f * (aD[1][k] + aD[2][k])) - m1;
+            else dm[k] = m1;
+        }
     }
     // right eigenvectors (S08 A12) applied to the limited amplitudes
     float sf = dm[0] + dm[5], df = dm[5] - dm[0];
@@ -377,10 +387,11 @@ __device__ __forceinline__ void riemann_flux(const T* uL, const T* uR, T cs, T a
     }
 }
 
-template <class T>
-__device__ __forceinline__ void char_slope(const T* wm, const T* w0, const T* wp, T bn, T cs, T asqr, T* delw) {
-    if constexpr (std::is_same<T, float>::value) plm_char_slope_fast(wm, w0, wp, bn, cs, asqr, delw);
-    else plm_char_slope(wm, w0, wp, bn, cs, asqr, delw);
+template <class T, bool PPM = false>
+__device__ __forceinline__ void char_slope(const T* wm, const T* w0, const T* wp, const T* wp2, T bn, T cs, T asqr,
+                                           T* delw) {
+    if constexpr (std::is_same<T, float>::value) plm_char_slope_fast<PPM>(wm, w0, wp, wp2, bn, cs, asqr, delw);
+    else plm_char_slope<T, PPM>(wm, w0, wp, wp2, bn, cs, asqr, delw);
 }
 
 }  // namespace imhd

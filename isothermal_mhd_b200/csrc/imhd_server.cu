@@ -121,7 +121,7 @@ bool valid_box(const imhd_config& c, std::string& why) {
     if (c.nx < 4 || c.ny < 4 || c.nz < 4) { why = "every edge needs at least 4 cells"; return false; }
     if ((double)c.nx * c.ny * c.nz >= 2147483647.0) { why = "box too large"; return false; }
     if (c.riemann < 1 || c.riemann > 3) { why = "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE"; return false; }
-    if (c.recon != IMHD_PLM) { why = "only IMHD_PLM reconstruction is implemented"; return false; }
+    if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) { why = "recon must be IMHD_PLM or IMHD_PPM"; return false; }
     if (c.npass < 0 || c.npass > imhd::kMaxPass) { why = "npass must be in 0..8"; return false; }
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) { why = "sound_speed and cour must be positive"; return false; }
     if (c.ng < 0 || c.ng_pass < 0) { why = "ghost widths must be >= 0"; return false; }
@@ -214,7 +214,7 @@ struct Worker {
     bool build(Resident& r) {
         const Request& q = r.req;
         const imhd_config& c = q.cfg;
-        imhd::init_rec(r.rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.sound_speed, c.cour, c.edot, c.dt_turb);
+        imhd::init_rec(r.rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
         r.bytes = imhd::box_bytes(r.rec, s->esz, q.forcing != 0);
         cudaError_t e = cudaMallocAsync(&r.mem, r.bytes, st);
         if (e != cudaSuccess) {
@@ -352,7 +352,7 @@ struct Worker {
                 if (s->queue.empty()) return true;
                 const Request& h = s->queue.front();
                 imhd::BoxRec probe;
-                imhd::init_rec(probe, h.cfg.nx, h.cfg.ny, h.cfg.nz, h.cfg.npass, h.cfg.riemann, h.cfg.sound_speed,
+                imhd::init_rec(probe, h.cfg.nx, h.cfg.ny, h.cfg.nz, h.cfg.npass, h.cfg.riemann, h.cfg.recon, h.cfg.sound_speed,
                                h.cfg.cour, h.cfg.edot, h.cfg.dt_turb);
                 size_t need = imhd::box_bytes(probe, s->esz, h.forcing != 0);
                 long long cells = (long long)h.cfg.nx * h.cfg.ny * h.cfg.nz;

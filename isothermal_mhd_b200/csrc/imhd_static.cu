@@ -105,7 +105,7 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     if (rc) return fail(rc, err);
 
     imhd::BoxRec rec;
-    imhd::init_rec(rec, nx, ny, nz, npass, riemann, sound_speed, cour, 0.0, 0.0);
+    imhd::init_rec(rec, nx, ny, nz, npass, riemann, IMHD_PLM, sound_speed, cour, 0.0, 0.0);
     rec.S[0] = const_cast<void*>(state_in);
     rec.S[1] = state_out;
     unsigned char* p = base;

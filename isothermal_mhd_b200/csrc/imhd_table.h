@@ -27,9 +27,9 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
     if (kind == kKindCell) return nbx * r.ny * r.nz;
     if (kind == kKindCellZ) return nbx * r.ny * ceil_div(r.nz, kSegZ);
     if (kind == kKindRed) return r.nred;
-    int solver = 1 + (kind - kKindSolver0) / 5;
+    int scheme = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
-    if (r.riemann != solver) return 0;
+    if (scheme_of(r.riemann, r.recon) != scheme) return 0;
     bool row = row_capable(r.nx, esz);
     switch (sub) {
         case kSubCell: return nbx * r.ny * r.nz;
@@ -72,11 +72,12 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
         bd.totals[k] = (int)acc;
     }
     bd.row_nx_max = 0;
-    for (int s = 0; s < 4; ++s) bd.has_solver[s] = false;
+    for (int s = 0; s <= kSchemes; ++s) bd.has_scheme[s] = false;
     bd.any_pass = false;
     bd.npass_max = 0;
     for (const BoxRec& r : recs) {
-        if (r.riemann >= 1 && r.riemann <= 3) bd.has_solver[r.riemann] = true;
+        if (r.riemann >= 1 && r.riemann <= 3 && (r.recon == 0 || r.recon == 1))
+            bd.has_scheme[scheme_of(r.riemann, r.recon)] = true;
         if (r.npass > 0) bd.any_pass = true;
         if (r.npass > bd.npass_max) bd.npass_max = r.npass;
         if (row_capable(r.nx, esz) && r.nx > bd.row_nx_max) bd.row_nx_max = r.nx;
@@ -145,12 +146,14 @@ inline void host_ghost_fill(int nx, int ny, int nz, double* h, int ng) {
 }
 
 // Fill the geometry fields of a box record from its configuration.
-inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, double cs, double cour, double edot,
+inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, int recon, double cs, double cour,
+                     double edot,
                      double dt_turb) {
     std::memset(&r, 0, sizeof(r));
     r.nx = nx; r.ny = ny; r.nz = nz; r.n = nx * ny * nz;
     r.npass = npass;
     r.riemann = riemann;
+    r.recon = recon;
     int pmax = ny * nz;
     if (nx * nz > pmax) pmax = nx * nz;
     if (nx * ny > pmax) pmax = nx * ny;

@@ -29,11 +29,17 @@ enum Stage {
 enum Kind {
     kKindCell = 0,     // ceil(nx/kBX) * ny * nz blocks of kBX threads, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
-    kKindSolver0 = 2,  // + 5*(solver-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another solver
-    kKindCellZ = 17,   // ceil(nx/kBX) * ny * ceil(nz/kSegZ) blocks of kBX threads, a z column of kSegZ cells per thread
-    kKinds = 18
+    kKindSolver0 = 2,  // + 5*(scheme-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
+    kKindCellZ = 32,   // ceil(nx/kBX) * ny * ceil(nz/kSegZ) blocks of kBX threads, a z column of kSegZ cells per thread
+    kKinds = 33
 };
-__host__ __device__ constexpr int solver_kind(int solver, int sub) { return kKindSolver0 + 5 * (solver - 1) + sub; }
+// A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
+// (0 PLM, 1 PPM): scheme = solver + 3 * recon, 1..kSchemes.
+constexpr int kSchemes = 6;
+__host__ __device__ constexpr int scheme_of(int solver, int recon) { return solver + 3 * recon; }
+__host__ __device__ constexpr int scheme_solver(int scheme) { return 1 + (scheme - 1) % 3; }
+__host__ __device__ constexpr int scheme_recon(int scheme) { return (scheme - 1) / 3; }
+__host__ __device__ constexpr int scheme_kind(int scheme, int sub) { return kKindSolver0 + 5 * (scheme - 1) + sub; }
 enum SolverSub { kSubCell = 0, kSubXRow = 1, kSubXTile = 2, kSubMarchY = 3, kSubMarchZ = 4 };
 
 // Device scalars of one box (FP64; maxima kept as the bit pattern of a
@@ -69,7 +75,7 @@ struct Scalars {
 struct BoxRec {
     int nx, ny, nz, n;
     int npass, riemann, plane_stride, nred;
-    int active, pad_;
+    int active, recon;      // running flag; 0 PLM, 1 PPM
     double dx, cs, cour, edot, dt_turb;
     void* S[2];
     void* F;        // 18 flux fields
@@ -99,7 +105,7 @@ struct BatchDev {
     BatchArgs a;               // device pointers
     int totals[kKinds];        // blocks per kind (grid sizes)
     int row_nx_max = 0;        // largest nx among boxes using the x-row sweep
-    bool has_solver[4] = {false, false, false, false};
+    bool has_scheme[kSchemes + 1] = {};
     bool any_pass = false;
     int npass_max = 0;         // largest passive count of the table
     int drive_mode = 0;        // 0: no forcing, 1: every box drives (host decided), 2: per-box device flags

@@ -77,7 +77,7 @@ class Server:
         """Queue the driven-turbulence box of a BoxSpec."""
         kv, av, sv, af, sf = spec.fields()
         cfg = make_config(spec.n, precision=self.precision, riemann=spec.riemann, npass=spec.npass, cour=cour,
-                          edot=spec.edot if forcing else 0.0, dt_turb=spec.dt_turb)
+                          edot=spec.edot if forcing else 0.0, dt_turb=spec.dt_turb, recon=spec.recon)
         return self.submit_raw(cfg, spec.steps, rho=1.0, b0=spec.b0, kvec=kv, amp_velocity=av, scale_velocity=sv,
                                amp_force=af if forcing else None, scale_force=sf, forcing=forcing)
 

@@ -37,6 +37,7 @@ class BoxSpec:
     seed: int = 0
     dt_turb: float = 0.05
     arrival: float = 0.0          # seconds after the start of a request stream
+    recon: str = "plm"
 
     @property
     def edot(self):

@@ -20,11 +20,11 @@ def rel_l1(a, b):
 
 
 def oracle_run(ic, n, riemann, steps, cour=0.4, npass=None, dt0=1e-15, force=None, drive_at=(), edot=1e-3,
-               dt_turb=0.05, nthreads=4):
+               dt_turb=0.05, nthreads=4, recon="plm"):
     from oracle.pyoracle import Oracle
     q, b, p = ic
     npass = p.shape[0] if npass is None else npass
-    o = Oracle(n, riemann=riemann, npass=npass, nthreads=nthreads)
+    o = Oracle(n, riemann=riemann, recon=recon, npass=npass, nthreads=nthreads)
     o.set_state(q, b, p if npass else None)
     if force is not None:
         o.set_force(force, edot=edot, dt_turb=dt_turb)
@@ -44,11 +44,12 @@ def oracle_run(ic, n, riemann, steps, cour=0.4, npass=None, dt0=1e-15, force=Non
 
 
 def gpu_run(ic, n, riemann, steps, precision=64, cour=0.4, npass=None, dt0=1e-15, force=None, drive_at=(),
-            edot=1e-3, dt_turb=0.05, dts=None, ng=0):
+            edot=1e-3, dt_turb=0.05, dts=None, ng=0, recon="plm"):
     from isothermal_mhd_b200 import Box
     q, b, p = ic
     npass = p.shape[0] if npass is None else npass
-    box = Box(n, precision=precision, riemann=riemann, npass=npass, cour=cour, edot=edot, dt_turb=dt_turb, ng=ng)
+    box = Box(n, precision=precision, riemann=riemann, recon=recon, npass=npass, cour=cour, edot=edot,
+              dt_turb=dt_turb, ng=ng)
     box.upload(problems.pad(q, ng), problems.pad(b, ng), problems.pad(p, ng) if npass else None)
     if force is not None:
         box.set_force(problems.pad(force, ng))

@@ -13,10 +13,12 @@ from isothermal_mhd_b200.batch import make_config
 pytestmark = pytest.mark.gpu
 
 CASES = [((16, 16, 16), "roe", 1, 6), ((24, 16, 20), "hlld", 2, 4), ((12, 12, 12), "hlle", 0, 8)]
+RECON = ["plm", "ppm", "plm"]      # a PPM box among PLM boxes
 
 
-def alone(n, riemann, npass, steps, precision, ic, edot=0.0, delv=None):
-    with Box(n, precision=precision, riemann=riemann, npass=npass, cour=0.4, edot=edot, dt_turb=0.03) as box:
+def alone(n, riemann, npass, steps, precision, ic, edot=0.0, delv=None, recon="plm"):
+    with Box(n, precision=precision, riemann=riemann, recon=recon, npass=npass, cour=0.4, edot=edot,
+             dt_turb=0.03) as box:
         box.upload(ic[0], ic[1], ic[2] if npass else None)
         rec = driver.run(box, t_end=1e30, maxsteps=steps + 1, forcing=(lambda: delv) if delv is not None else None,
                          dt_turb=0.03)
@@ -43,8 +45,8 @@ def test_batch_equals_each_box_alone(precision, driven):
     for n, s, np_, _ in CASES:
         f = forcing.OUForcing(n, seed=5)
         forces.append(f.field(rms=1.0) if driven else None)
-    cfgs = [make_config(n, precision=precision, riemann=s, npass=np_, cour=0.4, edot=edot, dt_turb=0.03)
-            for n, s, np_, _ in CASES]
+    cfgs = [make_config(n, precision=precision, riemann=s, npass=np_, cour=0.4, edot=edot, dt_turb=0.03, recon=r)
+            for (n, s, np_, _), r in zip(CASES, RECON)]
     with Batch(cfgs) as bt:
         for i, (ic, (n, s, np_, st)) in enumerate(zip(ics, CASES)):
             bt.upload(i, ic[0], ic[1], ic[2] if np_ else None)
@@ -56,7 +58,7 @@ def test_batch_equals_each_box_alone(precision, driven):
         for i, (ic, (n, s, np_, st)) in enumerate(zip(ics, CASES)):
             q, b, p = bt.download(i)
             clk = bt.clock(i)
-            qa, ba, pa, rec = alone(n, s, np_, st, precision, ic, edot=edot, delv=forces[i])
+            qa, ba, pa, rec = alone(n, s, np_, st, precision, ic, edot=edot, delv=forces[i], recon=RECON[i])
             q1, b1, p1 = batch_of_one(cfgs[i], ic, np_, st, forces[i], driven)
             assert np.array_equal(q, q1) and np.array_equal(b, b1), (i, np.max(np.abs(q - q1)))
             if np_:

@@ -71,6 +71,36 @@ def test_fp64_bit_exact_32_roe():
     assert_exact(g, o)
 
 
+@pytest.mark.parametrize("riemann", SOLVERS)
+def test_fp64_bit_exact_ppm_noncubic(riemann):
+    # PPM characteristic reconstruction (the reference default) on all sweeps
+    n = (16, 20, 24)
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, riemann, steps=5, recon="ppm")
+    g = gpu_run(ic, n, riemann, steps=5, recon="ppm")
+    assert_exact(g, o)
+
+
+@pytest.mark.parametrize("axis", [0, 2])
+def test_fp64_bit_exact_ppm_shock(axis):
+    # discontinuities switch on the PPM monotonicity constraints
+    n = 16
+    ic = problems.shock_tube(n, axis=axis, npass=1)
+    o = oracle_run(ic, n, "hlld", steps=8, recon="ppm")
+    g = gpu_run(ic, n, "hlld", steps=8, recon="ppm")
+    assert_exact(g, o)
+
+
+def test_fp32_ppm_close_to_fp64_oracle():
+    n = 24
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, "roe", steps=10, recon="ppm")
+    g = gpu_run(ic, n, "roe", steps=10, precision=32, recon="ppm", dts=o["dts"])
+    for name in ("q", "b", "p"):
+        err = rel_l1(g[name], o[name])
+        assert np.all(err <= 1e-5), (name, err)
+
+
 def test_fp64_padded_layout_matches_unpadded():
     n = 16
     ic = problems.smooth_wave_box(n, npass=1)
