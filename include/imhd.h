@@ -167,6 +167,39 @@ int imhd_fourier_field(imhd_box* box, int target, const int* kvec, const double*
  * turbulence initial condition on the device without a host upload. */
 int imhd_init_uniform(imhd_box* box, double rho, const double* b0);
 
+/* ---- output and restart files (io_mod.f90) --------------------------------
+ * Written from the box's current state on the device (the cell records are
+ * packed there) and read back into it.  double_prec selects REAL*8 output,
+ * otherwise SNGL (round to nearest REAL*4) as the reference's double_prec
+ * switch does.
+ *
+ * imhd_write_xyzcube: the xyzcube_rank=XYZ_dump=N.dat stream file
+ *   (io_mod.f90:249-277): per interior cell, i fastest, q(1..7) and, when
+ *   npass > 0, the first passive scalar.
+ * imhd_write_state_dump: the per-rank block of the parallel dump
+ *   (io_mod.f90:378-432): per cell q(1..7) and every passive scalar.
+ * imhd_write_cuts: the cut files of io_mod.f90:62-240 into directory dir,
+ *   named as the reference names them for rank (0,0,0); flags selects them;
+ *   riemann (IMHD_ROE/HLLD/HLLE) names the xcut file.
+ * imhd_write_restart / imhd_read_restart: restart_mhd_rank=XYZ.dat
+ *   (io_mod.f90:440-517), Fortran sequential unformatted records with
+ *   gfortran's record markers: t_sim, q_3d and bface_3d with ghost width nb
+ *   (6 in the reference), qpass_3d with ghost width nb - 2 when npass > 0,
+ *   dump_count and the forcing generator's seeds s1, s2, s3.  Reading checks
+ *   every record length against the box's shape. */
+#define IMHD_CUT_X 1
+#define IMHD_CUT_Y 2
+#define IMHD_CUT_Z 4
+#define IMHD_CUT_XYDIAG 8
+#define IMHD_CUT_YZDIAG 16
+#define IMHD_CUT_XYPLANE 32
+int imhd_write_xyzcube(imhd_box* box, const char* path, int double_prec);
+int imhd_write_state_dump(imhd_box* box, const char* path, int double_prec);
+int imhd_write_cuts(imhd_box* box, const char* dir, int dump, int flags, int riemann, int double_prec);
+int imhd_write_restart(imhd_box* box, const char* path, double t_sim, int nb, int dump_count, int s1, int s2, int s3);
+int imhd_read_restart(imhd_box* box, const char* path, int nb, double* t_sim, int* dump_count, int* s1, int* s2,
+                      int* s3);
+
 /* ---- batches: many independent periodic boxes advanced together --------
  * All boxes of a batch share precision and device; sizes, Riemann solvers,
  * passive counts and physics parameters may differ.  Every kernel launch of a

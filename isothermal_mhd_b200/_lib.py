@@ -27,6 +27,7 @@ EXPORTS = (
     "imhd_batch_launch_count", "imhd_batch_destroy",
     "imhd_server_default_config", "imhd_server_start", "imhd_server_submit", "imhd_server_poll",
     "imhd_server_stats", "imhd_server_stop", "imhd_server_destroy",
+    "imhd_write_xyzcube", "imhd_write_state_dump", "imhd_write_cuts", "imhd_write_restart", "imhd_read_restart",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -160,6 +161,17 @@ def lib():
         L.imhd_server_stop.restype = i
         L.imhd_server_destroy.argtypes = [vp]
         L.imhd_server_destroy.restype = None
+        cp = ctypes.c_char_p
+        L.imhd_write_xyzcube.argtypes = [vp, cp, i]
+        L.imhd_write_xyzcube.restype = i
+        L.imhd_write_state_dump.argtypes = [vp, cp, i]
+        L.imhd_write_state_dump.restype = i
+        L.imhd_write_cuts.argtypes = [vp, cp, i, i, i, i]
+        L.imhd_write_cuts.restype = i
+        L.imhd_write_restart.argtypes = [vp, cp, d, i, i, i, i, i]
+        L.imhd_write_restart.restype = i
+        L.imhd_read_restart.argtypes = [vp, cp, i, dp, ip, ip, ip, ip]
+        L.imhd_read_restart.restype = i
         _lib = L
     return _lib
 

@@ -33,6 +33,7 @@ UNITS = {
     "imhd_static.cu": [],
     "imhd_batch.cu": [],
     "imhd_server.cu": [],
+    "imhd_io.cu": [],
 }
 HEADERS = ["imhd_physics.cuh", "imhd_physics_fast.cuh", "imhd_types.cuh", "imhd_table.h", "imhd_kernels.cuh", "imhd_launch.cuh"]
 

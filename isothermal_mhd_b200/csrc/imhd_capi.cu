@@ -200,6 +200,66 @@ const char* set_last_error(int code, const char* msg) {
     g_err = msg;
     return g_err.c_str();
 }
+
+// Upload / download with explicit ghost widths (the C ABI uses the box's
+// configured widths; restart files use the reference's nb and nb - 2).
+int box_upload_padded(imhd_box* x, const double* q, const double* bface, const double* qpass, int ng, int ng_pass) {
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    for (int f = 0; f < 7; ++f)
+        if ((rc = upload_field(x, host_field(x, q, f, ng), ng, field_ptr(x, cur_state(x), f)))) return rc;
+    for (int f = 0; f < 3; ++f)
+        if ((rc = upload_field(x, host_field(x, bface, f, ng), ng, field_ptr(x, cur_state(x), 7 + f)))) return rc;
+    for (int f = 0; f < x->cfg.npass; ++f)
+        if ((rc = upload_field(x, host_field(x, qpass, f, ng_pass), ng_pass, field_ptr(x, cur_state(x), 10 + f))))
+            return rc;
+    return sync_and_check(x);
+}
+
+int box_download_padded(imhd_box* x, double* q, double* bface, double* qpass, int ng, int ng_pass) {
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    const imhd_config& c = x->cfg;
+    // the transfers of one field reuse the staging buffer, so each field is
+    // completed (stream-ordered) before the next conversion overwrites it
+    if (q)
+        for (int f = 0; f < 7; ++f) {
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), f), (double*)host_field(x, q, f, ng), ng))) return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (bface)
+        for (int f = 0; f < 3; ++f) {
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), 7 + f), (double*)host_field(x, bface, f, ng), ng)))
+                return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (qpass && c.npass > 0)
+        for (int f = 0; f < c.npass; ++f) {
+            if ((rc = download_field(x, field_ptr(x, cur_state(x), 10 + f), (double*)host_field(x, qpass, f, ng_pass),
+                                     ng_pass)))
+                return rc;
+            if ((rc = sync_and_check(x))) return rc;
+        }
+    if (q) for (int f = 0; f < 7; ++f) ghost_fill(c, (double*)host_field(x, q, f, ng), ng);
+    if (bface) for (int f = 0; f < 3; ++f) ghost_fill(c, (double*)host_field(x, bface, f, ng), ng);
+    if (qpass) for (int f = 0; f < c.npass; ++f) ghost_fill(c, (double*)host_field(x, qpass, f, ng_pass), ng_pass);
+    return IMHD_OK;
+}
+
+// The current state buffer of a box and what is needed to read it on the
+// box's stream (after the box's pending work).
+int box_state_view(imhd_box* x, const void** state, int* nx, int* ny, int* nz, int* npass, int* precision,
+                   cudaStream_t* st) {
+    CK(cudaSetDevice(x->cfg.device));
+    *state = cur_state(x);
+    *nx = x->cfg.nx;
+    *ny = x->cfg.ny;
+    *nz = x->cfg.nz;
+    *npass = x->cfg.npass;
+    *precision = x->cfg.precision;
+    *st = x->b.st;
+    return IMHD_OK;
+}
 }  // namespace imhd
 
 extern "C" {
@@ -290,45 +350,12 @@ void imhd_destroy(imhd_box* x) {
 int imhd_upload(imhd_box* x, const double* q, const double* bface, const double* qpass) {
     if (!x || !q || !bface) return fail(IMHD_E_ARG, "null argument");
     if (x->cfg.npass > 0 && !qpass) return fail(IMHD_E_ARG, "qpass is NULL but npass > 0");
-    CK(cudaSetDevice(x->cfg.device));
-    int rc;
-    for (int f = 0; f < 7; ++f)
-        if ((rc = upload_field(x, host_field(x, q, f, x->cfg.ng), x->cfg.ng, field_ptr(x, cur_state(x), f)))) return rc;
-    for (int f = 0; f < 3; ++f)
-        if ((rc = upload_field(x, host_field(x, bface, f, x->cfg.ng), x->cfg.ng, field_ptr(x, cur_state(x), 7 + f)))) return rc;
-    for (int f = 0; f < x->cfg.npass; ++f)
-        if ((rc = upload_field(x, host_field(x, qpass, f, x->cfg.ng_pass), x->cfg.ng_pass, field_ptr(x, cur_state(x), 10 + f))))
-            return rc;
-    return sync_and_check(x);
+    return imhd::box_upload_padded(x, q, bface, qpass, x->cfg.ng, x->cfg.ng_pass);
 }
 
 int imhd_download(imhd_box* x, double* q, double* bface, double* qpass) {
     if (!x) return fail(IMHD_E_ARG, "null argument");
-    CK(cudaSetDevice(x->cfg.device));
-    int rc;
-    const imhd_config& c = x->cfg;
-    // the transfers of one field reuse the staging buffer, so each field is
-    // completed (stream-ordered) before the next conversion overwrites it
-    if (q)
-        for (int f = 0; f < 7; ++f) {
-            if ((rc = download_field(x, field_ptr(x, cur_state(x), f), (double*)host_field(x, q, f, c.ng), c.ng))) return rc;
-            if ((rc = sync_and_check(x))) return rc;
-        }
-    if (bface)
-        for (int f = 0; f < 3; ++f) {
-            if ((rc = download_field(x, field_ptr(x, cur_state(x), 7 + f), (double*)host_field(x, bface, f, c.ng), c.ng))) return rc;
-            if ((rc = sync_and_check(x))) return rc;
-        }
-    if (qpass && c.npass > 0)
-        for (int f = 0; f < c.npass; ++f) {
-            if ((rc = download_field(x, field_ptr(x, cur_state(x), 10 + f), (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass)))
-                return rc;
-            if ((rc = sync_and_check(x))) return rc;
-        }
-    if (q) for (int f = 0; f < 7; ++f) ghost_fill(c, (double*)host_field(x, q, f, c.ng), c.ng);
-    if (bface) for (int f = 0; f < 3; ++f) ghost_fill(c, (double*)host_field(x, bface, f, c.ng), c.ng);
-    if (qpass) for (int f = 0; f < c.npass; ++f) ghost_fill(c, (double*)host_field(x, qpass, f, c.ng_pass), c.ng_pass);
-    return IMHD_OK;
+    return imhd::box_download_padded(x, q, bface, qpass, x->cfg.ng, x->cfg.ng_pass);
 }
 
 int imhd_set_force(imhd_box* x, const double* delv) {
