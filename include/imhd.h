@@ -97,6 +97,8 @@ int imhd_download(imhd_box* box, double* q, double* bface, double* qpass);
  * add_random_force dummy argument (turb_driver_mod.f90:398).  Replaces the
  * hand-over of delv_re produced by generate_rand_force (:197-391). */
 int imhd_set_force(imhd_box* box, const double* delv);
+/* The force field of the box, in the layout of imhd_set_force. */
+int imhd_get_force(imhd_box* box, double* delv);
 
 /* One time step of the reference driver loop for one rank: copy_velocity,
  * vanleer_solve_3d(dt, drive_next) (vanleer_mod.f90:279-426, incl.
@@ -160,6 +162,19 @@ int imhd_stage_times(imhd_box* box, double* ms, long long* count, int n, int res
  * (turb_driver_mod.f90:310-384) for generators whose amplitudes live on the
  * host, e.g. the Ornstein-Uhlenbeck forcing of isothermal_mhd_b200.forcing. */
 int imhd_fourier_field(imhd_box* box, int target, const int* kvec, const double* amp, int nmodes, double scale);
+
+/* The reference's turbulence force generator on the device
+ * (turb_driver_mod.f90:23-79, 104-126, 197-391).  imhd_init_turb seeds the
+ * taus88 generator (the reference's defaults are 1234, 5678, 9123,
+ * constants_mod.f90:23) and sets k_max (2 in the reference; must be
+ * < min(nx, ny, nz) / 2).  imhd_generate_force draws the next random
+ * spectrum (serially, on the host, in the reference's order), projects it
+ * solenoidal, and evaluates the separable inverse DFT on the device into the
+ * box's force field, as imhd_set_force would set it; the generator state
+ * advances, and imhd_turb_seeds reads it (for restart files). */
+int imhd_init_turb(imhd_box* box, int s1, int s2, int s3, int k_max);
+int imhd_generate_force(imhd_box* box);
+int imhd_turb_seeds(imhd_box* box, int* s1, int* s2, int* s3);
 
 /* Uniform state: density rho, zero momentum, cell-centre and face field
  * b0[3], passive scalars 0, as homogenous_stationary sets it up

@@ -28,6 +28,7 @@ EXPORTS = (
     "imhd_server_default_config", "imhd_server_start", "imhd_server_submit", "imhd_server_poll",
     "imhd_server_stats", "imhd_server_stop", "imhd_server_destroy",
     "imhd_write_xyzcube", "imhd_write_state_dump", "imhd_write_cuts", "imhd_write_restart", "imhd_read_restart",
+    "imhd_init_turb", "imhd_generate_force", "imhd_turb_seeds", "imhd_get_force",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -172,6 +173,14 @@ def lib():
         L.imhd_write_restart.restype = i
         L.imhd_read_restart.argtypes = [vp, cp, i, dp, ip, ip, ip, ip]
         L.imhd_read_restart.restype = i
+        L.imhd_init_turb.argtypes = [vp, i, i, i, i]
+        L.imhd_init_turb.restype = i
+        L.imhd_generate_force.argtypes = [vp]
+        L.imhd_generate_force.restype = i
+        L.imhd_turb_seeds.argtypes = [vp, ip, ip, ip]
+        L.imhd_turb_seeds.restype = i
+        L.imhd_get_force.argtypes = [vp, dp]
+        L.imhd_get_force.restype = i
         _lib = L
     return _lib
 

@@ -156,6 +156,26 @@ class Box:
         ``torch.cuda.current_stream().cuda_stream``); None restores the box's own."""
         check(lib().imhd_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
 
+    def init_turb(self, seeds=(1234, 5678, 9123), k_max=2):
+        """Seed the reference force generator (taus88) and set k_max."""
+        check(lib().imhd_init_turb(self._h, int(seeds[0]), int(seeds[1]), int(seeds[2]), int(k_max)))
+
+    def generate_force(self):
+        """Next reference force field (generate_rand_force) into the box."""
+        check(lib().imhd_generate_force(self._h))
+
+    def get_force(self):
+        """The force field (3, nz+2g, ny+2g, nx+2g) in FP64."""
+        g = self.cfg.ng
+        out = np.empty((3, self.cfg.nz + 2 * g, self.cfg.ny + 2 * g, self.cfg.nx + 2 * g))
+        check(lib().imhd_get_force(self._h, _dptr(out)))
+        return out
+
+    def turb_seeds(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().imhd_turb_seeds(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
     def init_uniform(self, rho=1.0, b0=(0.0, 0.0, 0.0)):
         """Density rho, zero momentum, uniform field b0, passive scalars 0."""
         b = np.ascontiguousarray(b0, dtype=np.float64)

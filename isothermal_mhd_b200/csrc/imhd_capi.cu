@@ -3,6 +3,8 @@
 // array layout, and the per-step call sequence.
 #include <cuda_runtime.h>
 
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -21,6 +23,9 @@ template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, in
 template <class T> cudaError_t run_ou_field(cudaStream_t, const BoxRec&, int, int, const int*, const double*, int,
                                             double);
 template <class T> cudaError_t run_init_uniform(cudaStream_t, const BoxRec&, int, double, const double*);
+template <class T> cudaError_t run_ref_force(cudaStream_t, const BoxRec&, int, const double*, const double*,
+                                             const double*, const double*, const double*, double*, double*, double*,
+                                             double*);
 }  // namespace imhd
 
 struct imhd_box {
@@ -37,6 +42,11 @@ struct imhd_box {
     cudaStream_t own_stream = nullptr;
     double stage_ms[imhd::kStages] = {};
     long long stage_n[imhd::kStages] = {};
+    // reference force generator: taus88 state, k_max and the unit wave
+    // vectors khat(0:k_max, 0:k_max, 0:k_max, 3)
+    uint32_t taus[3] = {0, 0, 0};
+    int turb_km = 0;
+    std::vector<double> khat;
 };
 
 namespace {
@@ -377,6 +387,20 @@ int imhd_set_force(imhd_box* x, const double* delv) {
     return IMHD_OK;
 }
 
+int imhd_get_force(imhd_box* x, double* delv) {
+    if (!x || !delv) return fail(IMHD_E_ARG, "null argument");
+    if (!x->have_force || !x->rec.delv) return fail(IMHD_E_STATE, "the box has no force field");
+    CK(cudaSetDevice(x->cfg.device));
+    int rc;
+    for (int f = 0; f < 3; ++f) {
+        double* h = (double*)host_field(x, delv, f, x->cfg.ng);
+        if ((rc = download_field(x, field_ptr(x, x->rec.delv, f), h, x->cfg.ng))) return rc;
+        if ((rc = sync_and_check(x))) return rc;
+        ghost_fill(x->cfg, h, x->cfg.ng);
+    }
+    return IMHD_OK;
+}
+
 int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
     if (!x) return fail(IMHD_E_ARG, "null argument");
     if (!(dt > 0.0)) return fail(IMHD_E_ARG, "dt must be positive");
@@ -466,6 +490,166 @@ int imhd_wave_speeds(imhd_box* x, double* smax, double* delv_max) {
 }
 
 long long imhd_launch_count(imhd_box* x) { return x ? x->b.launches : 0; }
+
+// ---- reference force generator (turb_driver_mod.f90) ---------------------
+namespace {
+
+// taus88 (turb_driver_mod.f90:104-126): three Tausworthe components with the
+// 32-bit masks 0xFFFFFFFE, 0xFFFFFFF8, 0xFFFFFFF0 and logical shifts; the
+// result is 0.5 + (signed 32-bit xor) * 2.3283064365e-10.
+double taus88(uint32_t* s) {
+    uint32_t b;
+    b = ((s[0] << 13) ^ s[0]) >> 19;
+    s[0] = ((s[0] & 0xFFFFFFFEu) << 12) ^ b;
+    b = ((s[1] << 2) ^ s[1]) >> 25;
+    s[1] = ((s[1] & 0xFFFFFFF8u) << 4) ^ b;
+    b = ((s[2] << 3) ^ s[2]) >> 11;
+    s[2] = ((s[2] & 0xFFFFFFF0u) << 17) ^ b;
+    int32_t x = (int32_t)(s[0] ^ (s[1] ^ s[2]));
+    return 0.5 + (double)x * 2.3283064365e-10;
+}
+
+double sqd(double v) { return v * v; }
+
+}  // namespace
+
+int imhd_init_turb(imhd_box* x, int s1, int s2, int s3, int k_max) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    const imhd_config& c = x->cfg;
+    int nmin = c.nx < c.ny ? c.nx : c.ny;
+    nmin = nmin < c.nz ? nmin : c.nz;
+    // turb_driver_mod.f90:31-35
+    if (k_max < 1 || k_max >= nmin / 2) return fail(IMHD_E_ARG, "k_max must be >= 1 and < min(nx, ny, nz) / 2");
+    x->taus[0] = (uint32_t)s1;
+    x->taus[1] = (uint32_t)s2;
+    x->taus[2] = (uint32_t)s3;
+    x->turb_km = k_max;
+    // khat (turb_driver_mod.f90:46-66) for kx, ky, kz = 1..k_max; the entries
+    // with a zero component are never assigned by the reference and are 0 here
+    const int m = k_max + 1;
+    x->khat.assign((size_t)m * m * m * 3, 0.0);
+    const double TWOPI = 8.0 * std::atan(1.0);
+    const double dx = x->rec.dx;
+    const double kx0 = TWOPI / ((double)c.nx * dx), ky0 = TWOPI / ((double)c.ny * dx), kz0 = TWOPI / ((double)c.nz * dx);
+    for (int kz = 1; kz <= k_max; ++kz)
+        for (int ky = 1; ky <= k_max; ++ky)
+            for (int kx = 1; kx <= k_max; ++kx) {
+                double kk = std::sqrt(sqd(kx * kx0) + sqd(ky * ky0) + sqd(kz * kz0));
+                double* h = &x->khat[(((size_t)kz * m + ky) * m + kx) * 3];
+                h[0] = kx0 * kx / kk;
+                h[1] = ky0 * ky / kk;
+                h[2] = kz0 * kz / kk;
+            }
+    return IMHD_OK;
+}
+
+int imhd_turb_seeds(imhd_box* x, int* s1, int* s2, int* s3) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    if (s1) *s1 = (int)x->taus[0];
+    if (s2) *s2 = (int)x->taus[1];
+    if (s3) *s3 = (int)x->taus[2];
+    return IMHD_OK;
+}
+
+// generate_rand_force (turb_driver_mod.f90:197-391) for one rank: the
+// spectrum on the host (serial taus88 draws, k^6 exp(-8k/k_pk) power,
+// solenoidal projection with khat, Hermitian mirror), the separable inverse
+// DFT on the device; the field lands in the box's force buffer.
+int imhd_generate_force(imhd_box* x) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    if (x->turb_km == 0) return fail(IMHD_E_STATE, "imhd_init_turb must come before imhd_generate_force");
+    CK(cudaSetDevice(x->cfg.device));
+    const imhd_config& c = x->cfg;
+    const int km = x->turb_km, nk = 2 * km, m = km + 1;
+    const double TWOPI = 8.0 * std::atan(1.0);
+    const double dx = x->rec.dx;
+    const double Lx = (double)c.nx * dx, Ly = (double)c.ny * dx, Lz = (double)c.nz * dx;
+    const double kx0 = TWOPI / Lx, ky0 = TWOPI / Ly, kz0 = TWOPI / Lz;
+    double Lmax = Lx > Ly ? Lx : Ly;
+    Lmax = Lmax > Lz ? Lmax : Lz;
+    const double k_pk = TWOPI / Lmax;
+    const double sol_frac = 1.0;                         // turb_driver_mod.f90:214
+    const double const_sol = std::sqrt(sol_frac);
+    const double const_comp = std::sqrt(2.0 * (1.0 - sol_frac));
+    // spectrum V[c][kz][ky][kx], k = -km..km-1 stored at k + km (the +km
+    // entries of the reference's arrays are never read by the transform)
+    std::vector<double> V((size_t)2 * 3 * nk * nk * nk, 0.0);
+    double* Vre = V.data();
+    double* Vim = V.data() + (size_t)3 * nk * nk * nk;
+    auto K = [&](int kx, int ky, int kz, int cc) { return (((size_t)cc * nk + (kz + km)) * nk + (ky + km)) * nk + (kx + km); };
+    for (int kz = 0; kz <= km - 1; ++kz)
+        for (int ky = 0; ky <= km - 1; ++ky)
+            for (int kx = 0; kx <= km - 1; ++kx) {
+                double kk = std::sqrt(sqd(kx * kx0) + sqd(ky * ky0) + sqd(kz * kz0));
+                double k3 = (kk * kk) * kk;                  // k**6 as (k*k*k)**2
+                double Pk = (k3 * k3) * std::exp(-8.0 * kk / k_pk);
+                double rn[6];
+                for (int r = 0; r < 6; ++r) rn[r] = taus88(x->taus);
+                double amp[3], ph[3], dre[3], dim[3];
+                for (int q = 0; q < 3; ++q) amp[q] = std::sqrt(-2.0 * Pk * std::log(rn[q]));
+                for (int q = 0; q < 3; ++q) ph[q] = TWOPI * rn[3 + q];
+                for (int q = 0; q < 3; ++q) {
+                    dre[q] = amp[q] * std::cos(ph[q]);
+                    dim[q] = amp[q] * std::sin(ph[q]);
+                }
+                const double* kh = &x->khat[(((size_t)kz * m + ky) * m + kx) * 3];
+                double dotre = kh[0] * dre[0] + kh[1] * dre[1] + kh[2] * dre[2];
+                double dotim = kh[0] * dim[0] + kh[1] * dim[1] + kh[2] * dim[2];
+                for (int q = 0; q < 3; ++q) {
+                    double cre = kh[q] * dotre, cim = kh[q] * dotim;
+                    double sre = dre[q] - cre, sim = dim[q] - cim;
+                    Vre[K(kx, ky, kz, q)] = const_sol * sre + const_comp * cre;
+                    Vim[K(kx, ky, kz, q)] = const_sol * sim + const_comp * cim;
+                    Vre[K(-kx, -ky, -kz, q)] = Vre[K(kx, ky, kz, q)];
+                    Vim[K(-kx, -ky, -kz, q)] = -Vim[K(kx, ky, kz, q)];
+                }
+            }
+    // twiddles cos/sin(theta0 * i * k), i = 1..n the reference's cell index
+    auto twiddles = [&](int n) {
+        std::vector<double> tw((size_t)2 * n * (nk - 1));
+        const double theta0 = TWOPI / (double)n;
+        for (int i = 1; i <= n; ++i)
+            for (int jj = -(km - 1); jj <= km - 1; ++jj) {
+                double theta = theta0 * (double)i * (double)jj;
+                tw[(size_t)(i - 1) * (nk - 1) + (jj + km - 1)] = std::cos(theta);
+                tw[(size_t)n * (nk - 1) + (size_t)(i - 1) * (nk - 1) + (jj + km - 1)] = std::sin(theta);
+            }
+        return tw;
+    };
+    std::vector<double> twx = twiddles(c.nx), twy = twiddles(c.ny), twz = twiddles(c.nz);
+    int rc;
+    if (!x->rec.delv) {
+        if (cudaMalloc(&x->rec.delv, 3 * (size_t)x->rec.n * x->esz) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(IMHD_E_NOMEM, "device allocation of the force field failed");
+        }
+        if ((rc = upload_table(x))) return rc;
+    }
+    const size_t nV = V.size(), nX = twx.size(), nY = twy.size(), nZ = twz.size();
+    const size_t n1 = (size_t)3 * nk * nk * c.nx, n2 = (size_t)3 * nk * c.ny * c.nx;
+    double* d = nullptr;
+    const size_t total = nV + nX + nY + nZ + 2 * n1 + 2 * n2;
+    CK(cudaMallocAsync((void**)&d, total * sizeof(double), x->b.st));
+    double* dV = d;
+    double* dX = dV + nV;
+    double* dY = dX + nX;
+    double* dZ = dY + nY;
+    double* s1 = dZ + nZ;
+    double* s2 = s1 + 2 * n1;
+    cudaError_t e = cudaMemcpyAsync(dV, V.data(), nV * 8, cudaMemcpyHostToDevice, x->b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dX, twx.data(), nX * 8, cudaMemcpyHostToDevice, x->b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dY, twy.data(), nY * 8, cudaMemcpyHostToDevice, x->b.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dZ, twz.data(), nZ * 8, cudaMemcpyHostToDevice, x->b.st);
+    if (e == cudaSuccess)
+        e = is64(x) ? imhd::run_ref_force<double>(x->b.st, x->rec, km, dV, dV + nV / 2, dX, dY, dZ, s1, s1 + n1, s2, s2 + n2)
+                    : imhd::run_ref_force<float>(x->b.st, x->rec, km, dV, dV + nV / 2, dX, dY, dZ, s1, s1 + n1, s2, s2 + n2);
+    x->b.launches += 3;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(x->b.st);   // host vectors stay alive until the copies end
+    cudaFreeAsync(d, x->b.st);
+    CK(e);
+    x->have_force = true;
+    return sync_and_check(x);
+}
 
 int imhd_init_uniform(imhd_box* x, double rho, const double* b0) {
     if (!x || !b0) return fail(IMHD_E_ARG, "null argument");

@@ -1326,6 +1326,79 @@ __global__ void __launch_bounds__(kBX) k_fourier_field(BoxRec r, int cur, int ta
     }
 }
 
+// Separable inverse DFT of the reference force generator
+// (turb_driver_mod.f90:313-384, direct_idft_1d :461-486), one axis per pass,
+// interior cells only.  A spectrum line of 2*km entries (k = -km..km-1) is
+// summed over k = -(km-1)..km-1 in that order with the twiddles cos/sin of
+// theta0 * i * k (i the 1-based cell index), tabulated on the host as
+// tw[i0 * (2km-1) + (k + km-1)] (cos) and tw[ntw + ...] (sin).
+__device__ __forceinline__ void idft_line(const double* __restrict__ re, const double* __restrict__ im, int stride,
+                                          const double* __restrict__ cs, const double* __restrict__ sn, int km,
+                                          double& ore, double& oim) {
+    ore = 0.0;
+    oim = 0.0;
+    for (int jj = -(km - 1); jj <= km - 1; ++jj) {
+        const double vr = re[(size_t)(jj + km) * stride], vi = im[(size_t)(jj + km) * stride];
+        const double c = cs[jj + km - 1], s = sn[jj + km - 1];
+        ore = ore + (vr * c + (-1.0) * vi * s);
+        oim = oim + (vi * c - (-1.0) * vr * s);
+    }
+}
+
+// pass 1: V[c][kz][ky][kx] (each of 2km) -> A1[c][kz][ky][x]
+static __global__ void k_idft_x(const double* __restrict__ Vre, const double* __restrict__ Vim,
+                                const double* __restrict__ tw, int ntw, int km, int nx, double* __restrict__ Are,
+                                double* __restrict__ Aim) {
+    const int nk = 2 * km;
+    const long long total = 3LL * nk * nk * nx;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int x = (int)(t % nx);
+        long long line = t / nx;               // (c, kz, ky)
+        const double* cs = tw + (size_t)x * (nk - 1);
+        double ore, oim;
+        idft_line(Vre + line * nk, Vim + line * nk, 1, cs, cs + ntw, km, ore, oim);
+        Are[t] = ore;
+        Aim[t] = oim;
+    }
+}
+// pass 2: A1[c][kz][ky][x] -> A2[c][kz][y][x]
+static __global__ void k_idft_y(const double* __restrict__ Are, const double* __restrict__ Aim,
+                                const double* __restrict__ tw, int ntw, int km, int nx, int ny,
+                                double* __restrict__ Bre, double* __restrict__ Bim) {
+    const int nk = 2 * km;
+    const long long total = 3LL * nk * ny * nx;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        int x = (int)(t % nx);
+        int y = (int)((t / nx) % ny);
+        long long ckz = t / ((long long)nx * ny);  // (c, kz)
+        const double* cs = tw + (size_t)y * (nk - 1);
+        const size_t base = (size_t)ckz * nk * nx + x;
+        double ore, oim;
+        idft_line(Are + base, Aim + base, nx, cs, cs + ntw, km, ore, oim);
+        Bre[t] = ore;
+        Bim[t] = oim;
+    }
+}
+// pass 3: A2[c][kz][y][x] -> delv[c][z][y][x] = Re * idft_pre
+template <class T>
+__global__ void k_idft_z(const double* __restrict__ Bre, const double* __restrict__ Bim,
+                         const double* __restrict__ tw, int ntw, int km, int nx, int ny, int nz, double idft_pre,
+                         T* __restrict__ delv) {
+    const int nk = 2 * km;
+    const long long plane = (long long)nx * ny;
+    const long long total = 3LL * nz * plane;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        long long xy = t % plane;
+        int z = (int)((t / plane) % nz);
+        int c = (int)(t / (plane * nz));
+        const double* cs = tw + (size_t)z * (nk - 1);
+        const size_t base = (size_t)c * nk * plane + xy;
+        double ore, oim;
+        idft_line(Bre + base, Bim + base, (int)plane, cs, cs + ntw, km, ore, oim);
+        delv[t] = (T)(ore * idft_pre);
+    }
+}
+
 // Uniform state of S[cur]: density rho, zero momentum, cell-centre and face
 // field b0, passive scalars 0 (the homogenous_stationary set-up of
 // init_domain_mod.f90:406-479 with a uniform field).

@@ -247,6 +247,25 @@ cudaError_t run_clocks(BatchDev& b, double* out) {
     return cudaGetLastError();
 }
 
+// The three inverse-DFT passes of the reference force field into r.delv.
+// V: 3 x (2km)^3 spectrum (re, im); tw*: per-axis twiddle tables of
+// n_axis x (2km-1) cos values followed by as many sin values; scratch: room
+// for 2 x 3 x 2km x max(2km, ny) x nx doubles, twice.
+template <class T>
+cudaError_t run_ref_force(cudaStream_t st, const BoxRec& r, int km, const double* Vre, const double* Vim,
+                          const double* twx, const double* twy, const double* twz, double* s1re, double* s1im,
+                          double* s2re, double* s2im) {
+    const int nk = 2 * km;
+    auto blocks = [](long long n) { long long b = (n + 255) / 256; return (int)(b > 65535 * 8 ? 65535 * 8 : b); };
+    k_idft_x<<<blocks(3LL * nk * nk * r.nx), 256, 0, st>>>(Vre, Vim, twx, r.nx * (nk - 1), km, r.nx, s1re, s1im);
+    k_idft_y<<<blocks(3LL * nk * r.ny * r.nx), 256, 0, st>>>(s1re, s1im, twy, r.ny * (nk - 1), km, r.nx, r.ny, s2re,
+                                                            s2im);
+    const double idft_pre = 1.0 / (double)((long)r.nx * r.ny * r.nz);
+    k_idft_z<T><<<blocks(3LL * r.nz * r.ny * r.nx), 256, 0, st>>>(s2re, s2im, twz, r.nz * (nk - 1), km, r.nx, r.ny,
+                                                                  r.nz, idft_pre, (T*)r.delv);
+    return cudaGetLastError();
+}
+
 template <class T>
 cudaError_t run_init_uniform(cudaStream_t st, const BoxRec& r, int cur, double rho, const double* b0) {
     int blocks = (r.n + kBX - 1) / kBX;
@@ -268,4 +287,7 @@ cudaError_t run_init_uniform(cudaStream_t st, const BoxRec& r, int cur, double r
                                          double);                                  \
     template cudaError_t run_init_uniform<T>(cudaStream_t, const BoxRec&, int, double, const double*); \
     template cudaError_t run_clocks<T>(BatchDev&, double*);                       \
+    template cudaError_t run_ref_force<T>(cudaStream_t, const BoxRec&, int, const double*, const double*, \
+                                          const double*, const double*, const double*, double*, double*, \
+                                          double*, double*);                       \
     }

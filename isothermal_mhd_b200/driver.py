@@ -21,14 +21,18 @@ class RunRecord:
     drive_steps: list = field(default_factory=list)
 
 
-def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, record_dt=True, on_step=None):
+def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, record_dt=True, on_step=None,
+        seeds=(1234, 5678, 9123), k_max=2):
     """Advance `box` like the reference's main loop; returns a RunRecord.
 
     maxsteps follows the reference's counter: tsteps starts at 1 and the loop
     runs while tsteps < maxsteps, so maxsteps = N + 1 gives N steps.
     `forcing` is a callable returning the next delv field (3, nz+2g, ny+2g,
-    nx+2g), "device" for a force field already on the device (set by
-    Box.fourier_field; every drive reuses it), or None for an undriven run.
+    nx+2g), "ref" for the reference's generator on the device (seeded with
+    `seeds`, a new field before the run and after every drive step, as
+    driver.f90:336-339 and :102-105), "device" for a force field already on
+    the device (set by Box.fourier_field; every drive reuses it), or None for
+    an undriven run.
     """
     rec = RunRecord(t=t0)
     t_sim = t0
@@ -37,8 +41,12 @@ def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, r
     dt_turb = box.cfg.dt_turb if dt_turb is None else dt_turb
     t_turb = t_sim + dt_turb
     host_field = callable(forcing)
+    ref = forcing == "ref"
     if host_field:
         box.set_force(forcing())
+    if ref:
+        box.init_turb(seeds, k_max)
+        box.generate_force()
     while t_sim < t_end and tsteps < maxsteps:
         t_old = t_sim
         drive_next = False
@@ -55,6 +63,8 @@ def run(box, t_end, maxsteps, dt0=1.0e-15, forcing=None, dt_turb=None, t0=0.0, r
         tsteps += 1
         if drive_next and host_field:
             box.set_force(forcing())
+        if drive_next and ref:
+            box.generate_force()
         my_dt = min(t_end - t_sim, dt_new)
         if on_step is not None:
             on_step(tsteps, t_sim, my_dt)

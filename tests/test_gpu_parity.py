@@ -164,3 +164,56 @@ def test_uniform_state_stays_uniform_fp32_128():
     np.testing.assert_array_equal(qg, q.astype(np.float32).astype(np.float64))
     np.testing.assert_array_equal(bg, b.astype(np.float32).astype(np.float64))
     np.testing.assert_array_equal(pg, p.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("n", [16, (16, 12, 20)])
+def test_reference_force_generator_matches_oracle(n):
+    # generate_rand_force on the device: same taus88 draws, spectrum and
+    # separable inverse DFT as the oracle, FP64 bit for bit, three fields in a row
+    from oracle.pyoracle import Oracle
+    from isothermal_mhd_b200 import Box
+    o = Oracle(n, riemann="roe", npass=0)
+    ref = [o.generate_ref_force(seeds=(1234, 5678, 9123))]
+    ref += [o.generate_ref_force(init=False) for _ in range(2)]
+    o.close()
+    with Box(n, precision=64, riemann="roe", npass=0) as box:
+        box.init_turb((1234, 5678, 9123), k_max=2)
+        for r in ref:
+            box.generate_force()
+            np.testing.assert_array_equal(box.get_force(), r)
+        seeds = box.turb_seeds()
+    assert seeds != (1234, 5678, 9123)
+
+
+def test_driven_run_with_device_reference_generator_matches_oracle():
+    # driver loop with generate_rand_force before the run and after each drive
+    # (driver.f90:336-339, 102-105); drive-step sums differ in order only
+    from oracle.pyoracle import Oracle
+    from isothermal_mhd_b200 import Box, driver
+    n, steps, dt_turb, edot = 16, 12, 0.03, 0.5
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = Oracle(n, riemann="hlld", npass=1, nthreads=4)
+    o.set_state(*ic)
+    delv = o.generate_ref_force(seeds=(1234, 5678, 9123))
+    o.set_force(delv, edot=edot, dt_turb=dt_turb)
+    t, dt, t_turb, drives = 0.0, 1e-15, dt_turb, []
+    for s in range(steps):
+        drive = t_turb > t and t_turb <= t + dt
+        if drive:
+            t_turb = max(t_turb + dt_turb, t + 1e-2 * dt)
+            dt = 0.5 * dt
+            drives.append(s + 1)
+        cmax = o.step(dt, drive)
+        t += dt
+        if drive:
+            o.set_force(o.generate_ref_force(init=False), edot=edot, dt_turb=dt_turb)
+        dt = (0.5 if drive else 1.0) * 0.4 * o.dx / cmax
+    qo, bo, po = o.get_state()
+    o.close()
+    with Box(n, precision=64, riemann="hlld", npass=1, cour=0.4, edot=edot, dt_turb=dt_turb) as box:
+        box.upload(*ic)
+        rec = driver.run(box, t_end=1e30, maxsteps=steps + 1, forcing="ref", dt_turb=dt_turb)
+        qg, bg, pg = box.download()
+    assert rec.drive_steps == drives and len(drives) >= 2
+    for g, r in ((qg, qo), (bg, bo), (pg, po)):
+        assert np.all(rel_l1(g, r) <= 1e-12), rel_l1(g, r)
