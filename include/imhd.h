@@ -182,6 +182,25 @@ int imhd_turb_seeds(imhd_box* box, int* s1, int* s2, int* s3);
  * turbulence initial condition on the device without a host upload. */
 int imhd_init_uniform(imhd_box* box, double rho, const double* b0);
 
+/* ---- one box split over ranks: z slabs with halo planes ------------------
+ * A rank's slab is a box of nz_local + 2*H planes whose planes [H, H+nz_local)
+ * are its own and whose H planes on each side are copies of the neighbours'
+ * (the reference's halo exchange, mpi_domain_mod.f90:618-649, 674-3091).  A
+ * step runs over the whole slab with the periodic wrap in z, which corrupts
+ * only the outer planes: with H >= 6 (the reference's nb, enough for PLM and
+ * PPM) the own planes come out exact, and one exchange per step refreshes
+ * the halo.  imhd_set_geometry gives the global dx (1 / max global edge) and
+ * the own plane range [zlo, zhi): only those planes enter the step's speed
+ * maxima, floor counts, status, CFL and diagnostics, so the maxima over ranks
+ * equal the single-box ones.  imhd_pack_planes / imhd_unpack_planes copy
+ * planes [z0, z0 + nplanes) of every state field to / from a contiguous
+ * device buffer (field-major, (10 + npass) * nplanes * nx * ny elements of
+ * the box's precision) for the exchange; both return when the copy is done.
+ * Forcing across ranks needs global sums and is not offered on slabs. */
+int imhd_set_geometry(imhd_box* box, double dx, int zlo, int zhi);
+int imhd_pack_planes(imhd_box* box, int z0, int nplanes, void* dst);
+int imhd_unpack_planes(imhd_box* box, int z0, int nplanes, const void* src);
+
 /* ---- output and restart files (io_mod.f90) --------------------------------
  * Written from the box's current state on the device (the cell records are
  * packed there) and read back into it.  double_prec selects REAL*8 output,

@@ -164,6 +164,24 @@ class Box:
         """Next reference force field (generate_rand_force) into the box."""
         check(lib().imhd_generate_force(self._h))
 
+    def set_geometry(self, dx, zlo, zhi):
+        """Global cell size and the own z planes [zlo, zhi) of a slab."""
+        check(lib().imhd_set_geometry(self._h, float(dx), int(zlo), int(zhi)))
+
+    def pack_planes(self, z0, nplanes, out=None):
+        """Planes [z0, z0+nplanes) of every state field as a flat uint8 CUDA
+        tensor (field-major), for halo exchange."""
+        import torch
+        esz = 8 if self.cfg.precision == 64 else 4
+        nbytes = (10 + self.cfg.npass) * nplanes * self.cfg.nx * self.cfg.ny * esz
+        if out is None:
+            out = torch.empty(nbytes, dtype=torch.uint8, device=torch.device("cuda", self.cfg.device))
+        check(lib().imhd_pack_planes(self._h, int(z0), int(nplanes), ctypes.c_void_p(out.data_ptr())))
+        return out
+
+    def unpack_planes(self, z0, nplanes, src):
+        check(lib().imhd_unpack_planes(self._h, int(z0), int(nplanes), ctypes.c_void_p(src.data_ptr())))
+
     def get_force(self):
         """The force field (3, nz+2g, ny+2g, nx+2g) in FP64."""
         g = self.cfg.ng

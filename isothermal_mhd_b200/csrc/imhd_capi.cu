@@ -651,6 +651,43 @@ int imhd_generate_force(imhd_box* x) {
     return sync_and_check(x);
 }
 
+int imhd_set_geometry(imhd_box* x, double dx, int zlo, int zhi) {
+    if (!x) return fail(IMHD_E_ARG, "null argument");
+    if (!(dx > 0.0)) return fail(IMHD_E_ARG, "dx must be positive");
+    if (zlo < 0 || zhi > x->cfg.nz || zlo >= zhi) return fail(IMHD_E_ARG, "need 0 <= zlo < zhi <= nz");
+    CK(cudaSetDevice(x->cfg.device));
+    x->rec.dx = dx;
+    x->rec.zlo = zlo;
+    x->rec.zhi = zhi;
+    return upload_table(x);
+}
+
+int imhd_pack_planes(imhd_box* x, int z0, int nplanes, void* dst) {
+    if (!x || !dst) return fail(IMHD_E_ARG, "null argument");
+    if (z0 < 0 || nplanes < 0 || z0 + nplanes > x->cfg.nz) return fail(IMHD_E_ARG, "plane range outside the box");
+    CK(cudaSetDevice(x->cfg.device));
+    const size_t plane = (size_t)x->cfg.nx * x->cfg.ny * x->esz;
+    const int nf = 10 + x->cfg.npass;
+    for (int f = 0; f < nf; ++f)
+        CK(cudaMemcpyAsync((char*)dst + (size_t)f * nplanes * plane,
+                           (const char*)field_ptr(x, cur_state(x), f) + (size_t)z0 * plane, (size_t)nplanes * plane,
+                           cudaMemcpyDeviceToDevice, x->b.st));
+    return sync_and_check(x);
+}
+
+int imhd_unpack_planes(imhd_box* x, int z0, int nplanes, const void* src) {
+    if (!x || !src) return fail(IMHD_E_ARG, "null argument");
+    if (z0 < 0 || nplanes < 0 || z0 + nplanes > x->cfg.nz) return fail(IMHD_E_ARG, "plane range outside the box");
+    CK(cudaSetDevice(x->cfg.device));
+    const size_t plane = (size_t)x->cfg.nx * x->cfg.ny * x->esz;
+    const int nf = 10 + x->cfg.npass;
+    for (int f = 0; f < nf; ++f)
+        CK(cudaMemcpyAsync((char*)field_ptr(x, cur_state(x), f) + (size_t)z0 * plane,
+                           (const char*)src + (size_t)f * nplanes * plane, (size_t)nplanes * plane,
+                           cudaMemcpyDeviceToDevice, x->b.st));
+    return sync_and_check(x);
+}
+
 int imhd_init_uniform(imhd_box* x, double rho, const double* b0) {
     if (!x || !b0) return fail(IMHD_E_ARG, "null argument");
     if (!(rho > 0.0)) return fail(IMHD_E_ARG, "rho must be positive");

@@ -190,7 +190,8 @@ __global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
         uR[3] = fld(S, R::MT2, dm.n)[cn]; uR[4] = uL[4];
         uR[5] = fld(S, R::BT1, dm.n)[cn]; uR[6] = fld(S, R::BT2, dm.n)[cn];
         T Fo[7];
-        riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, smax);
+        T sdrop = T(0);     // faces outside zlo..zhi-1 do not enter smax
+        riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
         T* Fd = F + (size_t)(6 * D) * dm.n;
         Fd[c] = Fo[0];
         Fd[(size_t)dm.n + c] = Fo[1];
@@ -285,7 +286,9 @@ __global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
                 T qL[7], qR[7], Fo[7];
                 plm_left_state(wb_, dA, bnA, qL);
                 plm_right_state(wc, dB, bnA, qR);
-                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+                const int kf = (D == 1) ? o : a;
+                T sdrop = T(0);
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop);
                 store_flux(F, D, dm.n, base + a * stride, Fo);
 #pragma unroll
                 for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
@@ -315,7 +318,9 @@ __global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
                 T qL[7], qR[7], Fo[7];
                 ppm_state(r0, bn0, qL);
                 ppm_state(l1, bn0, qR);
-                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+                const int kf = (D == 1) ? o : a;
+                T sdrop = T(0);
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop);
                 store_flux(F, D, dm.n, base + a * stride, Fo);
 #pragma unroll
                 for (int m = 0; m < 6; ++m) {
@@ -409,7 +414,8 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
             ppm_state(r, bn, qL);
             ppm_state(l1, bn, qR);
         }
-        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+        T sdrop = T(0);
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
     block_atomic_max<TX>(smax_slots, (double)smax);
@@ -494,7 +500,8 @@ __global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
             ppm_state(r, bn, qL);
             ppm_state(l1, bn, qR);
         }
-        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, smax);
+        T sdrop = T(0);
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
         store_flux(F, 0, dm.n, row + i, Fo);
     }
     block_atomic_max_any(smax_slots, (double)smax);
@@ -688,7 +695,9 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
 // A thread walks a column of kSegZ cells along z; the z-face fluxes, the
 // corner EMFs at k and the new face field bz read or computed at plane k are
 // the "k-1" values of plane k+1 and are carried instead of reloaded.
-template <class T, bool ONE>
+// ZR: some box of the table restricts its maxima to a z range (slabs); the
+// other instantiation has no per-plane test on the hot path.
+template <class T, bool ONE, bool ZR>
 __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArgs ba, double dt_scale, int final_stage) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
@@ -748,9 +757,10 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArg
                 Fz0[v] = F[(size_t)(12 + fz) * n + c];
                 out[v] = fld(S0, v, n)[c] - dtdx * ((Fx[c] - Fx[cxm]) + (Fy[c] - Fy[cym]) + (Fz0[v] - Fzm[v]));
             }
+            const bool inz = !ZR || (k >= rp.zlo && k < rp.zhi);
             if (out[0] < T(kMIN_DENS)) {
                 out[0] = T(kMIN_DENS);
-                atomicAdd(floor_hits, 1ull);
+                if (inz) atomicAdd(floor_hits, 1ull);
             }
             const T Ex0 = Ex[c], Ey0 = Ey[c], Ez0 = E[2 * (size_t)n + c];
             const T Ex_ym = Ex[cym], Ey_xm = Ey[cxm];
@@ -772,9 +782,10 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArg
             fld(Sout, 7, n)[c] = bx;
             fld(Sout, 8, n)[c] = by;
             fld(Sout, 9, n)[c] = bz;
-            if (do_cfl) cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
-            if (!(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
-                  isfinite(by) && isfinite(bz)))
+            if (do_cfl && inz)
+                cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
+            if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
+                         isfinite(by) && isfinite(bz)))
                 atomicOr(status, 2u);
 #pragma unroll
             for (int v = 0; v < 4; ++v) Fzm[v] = Fz0[v];
@@ -1006,7 +1017,10 @@ __global__ void __launch_bounds__(kRedThreads) k_force_sums(BatchArgs ba) {
     double* __restrict__ partials = rp.partials;
     const int n = rp.n;
     double s[5] = {0, 0, 0, 0, 0};
+    const int plane = rp.nx * rp.ny;
     for (int c = local * blockDim.x + threadIdx.x; c < n; c += rp.nred * blockDim.x) {
+        const int kc = c / plane;
+        if (kc < rp.zlo || kc >= rp.zhi) continue;
         double rho = (double)fld(S0, 0, n)[c];
         double d1 = (double)delv[c], d2 = (double)delv[(size_t)n + c], d3 = (double)delv[2 * (size_t)n + c];
         s[0] += rho * (d1 * d1 + d2 * d2 + d3 * d3);
@@ -1092,6 +1106,7 @@ __global__ void __launch_bounds__(kBX) k_force_kick(BatchArgs ba) {
     int i, j, k;
     decode_cell<ONE>(local, dm, i, j, k);
     bool valid = i < dm.nx;
+    const bool inz = k >= rp.zlo && k < rp.zhi;
     double dvmax = 0.0, cmax = 0.0;
     if (valid) {
         const int n = dm.n;
@@ -1120,8 +1135,8 @@ __global__ void __launch_bounds__(kBX) k_force_kick(BatchArgs ba) {
         fld(S1, 1, n)[c] = mx;
         fld(S1, 2, n)[c] = my;
         fld(S1, 3, n)[c] = mz;
-        dvmax = vmax(vmax(vmax(dvmax, fabs(dmx) / r0), fabs(dmy) / r0), fabs(dmz) / r0);
-        cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
+        if (inz) dvmax = vmax(vmax(vmax(dvmax, fabs(dmx) / r0), fabs(dmy) / r0), fabs(dmz) / r0);
+        if (inz) cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
                                       fld(S1, 6, n)[c], asqr);
     }
     block_atomic_max<kBX>(sc->dvmax_slots, dvmax);
@@ -1223,7 +1238,7 @@ __global__ void __launch_bounds__(kBX) k_cfl(BatchArgs ba) {
     int i, j, k;
     decode_cell<ONE>(local, dm, i, j, k);
     double cm = 0.0;
-    if (i < dm.nx) {
+    if (i < dm.nx && k >= rp.zlo && k < rp.zhi) {
         const int n = dm.n;
         int c = i + dm.nx * (j + dm.ny * k);
         cm = (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],
@@ -1246,6 +1261,7 @@ __global__ void __launch_bounds__(kRedThreads) k_diag(BatchArgs ba) {
     double s[6] = {0, 0, 0, 0, 0, 0};
     for (int c = local * blockDim.x + threadIdx.x; c < n; c += rp.nred * blockDim.x) {
         int i = c % dm.nx, j = (c / dm.nx) % dm.ny, k = c / (dm.nx * dm.ny);
+        if (k < rp.zlo || k >= rp.zhi) continue;
         double rho = vmin(vmax((double)fld(S, 0, n)[c], 1.0e-15), 1.0e10);
         double mx = (double)fld(S, 1, n)[c], my = (double)fld(S, 2, n)[c], mz = (double)fld(S, 3, n)[c];
         double vsqr = vmin((mx * mx + my * my + mz * mz) / (rho * rho), 1.0e5);

@@ -141,7 +141,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStPredEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
     mark(b, kStPredUpdate);
-    k_update<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
+    if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
+    else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
     b.launches += 2;
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
@@ -154,7 +155,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStCorrEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
     mark(b, kStFinalUpdate);
-    k_update<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
+    if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
+    else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
     b.launches += 2;
     if (b.drive_mode) {
         mark(b, kStForceKick);

@@ -75,11 +75,13 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
     for (int s = 0; s <= kSchemes; ++s) bd.has_scheme[s] = false;
     bd.any_pass = false;
     bd.npass_max = 0;
+    bd.any_zrange = false;
     for (const BoxRec& r : recs) {
         if (r.riemann >= 1 && r.riemann <= 3 && (r.recon == 0 || r.recon == 1))
             bd.has_scheme[scheme_of(r.riemann, r.recon)] = true;
         if (r.npass > 0) bd.any_pass = true;
         if (r.npass > bd.npass_max) bd.npass_max = r.npass;
+        if (r.zlo != 0 || r.zhi != r.nz) bd.any_zrange = true;
         if (row_capable(r.nx, esz) && r.nx > bd.row_nx_max) bd.row_nx_max = r.nx;
     }
     bd.a.nbox = nbox;
@@ -154,6 +156,8 @@ inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, 
     r.npass = npass;
     r.riemann = riemann;
     r.recon = recon;
+    r.zlo = 0;
+    r.zhi = nz;
     int pmax = ny * nz;
     if (nx * nz > pmax) pmax = nx * nz;
     if (nx * ny > pmax) pmax = nx * ny;

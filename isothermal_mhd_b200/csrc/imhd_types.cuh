@@ -76,6 +76,8 @@ struct BoxRec {
     int nx, ny, nz, n;
     int npass, riemann, plane_stride, nred;
     int active, recon;      // running flag; 0 PLM, 1 PPM
+    int zlo, zhi;           // z planes whose cells and faces enter the step's maxima and sums
+    int pad2_[2];
     double dx, cs, cour, edot, dt_turb;
     void* S[2];
     void* F;        // 18 flux fields
@@ -108,6 +110,7 @@ struct BatchDev {
     bool has_scheme[kSchemes + 1] = {};
     bool any_pass = false;
     int npass_max = 0;         // largest passive count of the table
+    bool any_zrange = false;   // some box restricts its maxima to a z range
     int drive_mode = 0;        // 0: no forcing, 1: every box drives (host decided), 2: per-box device flags
     int precision = 64;
     cudaStream_t st = nullptr;
