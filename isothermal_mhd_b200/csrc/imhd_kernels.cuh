@@ -53,39 +53,45 @@ __device__ __forceinline__ BoxRec resolve(const BatchArgs& ba, int kind, int& lo
 // Box b of the table (the kernels that run one thread or block per box).
 __device__ __forceinline__ BoxRec box_at(const BatchArgs& ba, int b) { return ba.use_one ? ba.one : ba.boxes[b]; }
 __device__ __forceinline__ Dims dims_of(const BoxRec& r) { return Dims{r.nx, r.ny, r.nz, r.n}; }
-// kKindCell decomposition: ceil(nx/kBX) blocks per (j,k) row
-// (a single box launches a 3D grid (nbx, ny, nz) and needs no division)
+// kKindCell decomposition: (x, y) tiles of (1 << tws) x (kBX >> tws)
+// threads per z plane (a single box launches the 3D grid (nbx, nby, nz) and
+// needs no division).  j may exceed ny - 1 in the last tile row: callers test
+// i < nx and j < ny.
 template <bool ONE>
-__device__ __forceinline__ void decode_cell(int local, const Dims& dm, int& i, int& j, int& k) {
+__device__ __forceinline__ void decode_cell(int local, const Dims& dm, int tws, int& i, int& j, int& k) {
+    const int tw = 1 << tws, th = kBX >> tws;
+    const int lx = (int)threadIdx.x & (tw - 1), ly = (int)threadIdx.x >> tws;
     if constexpr (ONE) {
-        i = (int)(blockIdx.x * kBX + threadIdx.x);
-        j = (int)blockIdx.y;
+        i = (int)blockIdx.x * tw + lx;
+        j = (int)blockIdx.y * th + ly;
         k = (int)blockIdx.z;
     } else {
-        int nbx = (dm.nx + kBX - 1) / kBX;
+        int nbx = (dm.nx + tw - 1) >> tws, nby = (dm.ny + th - 1) / th;
         int bx = local % nbx, rest = local / nbx;
-        j = rest % dm.ny;
-        k = rest / dm.ny;
-        i = bx * kBX + (int)threadIdx.x;
+        i = bx * tw + lx;
+        j = (rest % nby) * th + ly;
+        k = rest / nby;
     }
 }
 
-// kKindCellZ decomposition: ceil(nx/kBX) blocks per (j, z segment); the
-// thread's column is k0 <= k < k1 (a single box launches a 3D grid
-// (nbx, ny, nseg))
+// kKindCellZ decomposition: the same tiles per z segment; the thread's column
+// is k0 <= k < k1 (a single box launches a 3D grid (nbx, nby, nseg)).
+// Callers test i < nx and j < ny.
 template <bool ONE>
-__device__ __forceinline__ void decode_cellz(int local, const Dims& dm, int& i, int& j, int& k0, int& k1) {
+__device__ __forceinline__ void decode_cellz(int local, const Dims& dm, int tws, int& i, int& j, int& k0, int& k1) {
+    const int tw = 1 << tws, th = kBX >> tws;
+    const int lx = (int)threadIdx.x & (tw - 1), ly = (int)threadIdx.x >> tws;
     int seg;
     if constexpr (ONE) {
-        i = (int)(blockIdx.x * kBX + threadIdx.x);
-        j = (int)blockIdx.y;
+        i = (int)blockIdx.x * tw + lx;
+        j = (int)blockIdx.y * th + ly;
         seg = (int)blockIdx.z;
     } else {
-        int nbx = (dm.nx + kBX - 1) / kBX;
+        int nbx = (dm.nx + tw - 1) >> tws, nby = (dm.ny + th - 1) / th;
         int bx = local % nbx, rest = local / nbx;
-        j = rest % dm.ny;
-        seg = rest / dm.ny;
-        i = bx * kBX + (int)threadIdx.x;
+        i = bx * tw + lx;
+        j = (rest % nby) * th + ly;
+        seg = rest / nby;
     }
     k0 = seg * kSegZ;
     k1 = min(k0 + kSegZ, dm.nz);
@@ -173,8 +179,8 @@ __global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
     const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
     unsigned long long* smax_slots = sc->smax_slots;
     int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
-    bool valid = i < dm.nx;
+    decode_cell<ONE>(local, dm, rp.tws, i, j, k);
+    bool valid = i < dm.nx && j < dm.ny;
     T smax = T(0);
     if (valid) {
         int c = i + dm.nx * (j + dm.ny * k);
@@ -250,21 +256,24 @@ __global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
     const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
     unsigned long long* smax_slots = sc->smax_slots;
     const int seg = kSeg;
-    int bx, o, a0;                              // o: k for D=1, j for D=2
-    if constexpr (ONE) {                        // grid (nbx, nother, nseg)
-        bx = (int)blockIdx.x; o = (int)blockIdx.y; a0 = (int)blockIdx.z * seg;
+    // (x, other) tiles of the box's shape, other = z for D=1 and y for D=2
+    const int nother = (D == 1) ? dm.nz : dm.ny;
+    const int tw = 1 << rp.tws, th = kBX >> rp.tws;
+    int bx, bo, a0;
+    if constexpr (ONE) {                        // grid (nbx, nbo, nseg)
+        bx = (int)blockIdx.x; bo = (int)blockIdx.y; a0 = (int)blockIdx.z * seg;
     } else {
-        int nbx = (dm.nx + kBX - 1) / kBX;
-        int nother = (D == 1) ? dm.nz : dm.ny;
+        int nbx = (dm.nx + tw - 1) >> rp.tws, nbo = (nother + th - 1) / th;
         int rest = local / nbx;
         bx = local % nbx;
-        o = rest % nother;
-        a0 = (rest / nother) * seg;
+        bo = rest % nbo;
+        a0 = (rest / nbo) * seg;
     }
-    int i = bx * kBX + (int)threadIdx.x;
+    const int i = bx * tw + ((int)threadIdx.x & (tw - 1));
+    const int o = bo * th + ((int)threadIdx.x >> rp.tws);   // k for D=1, j for D=2
     int na = (D == 1) ? dm.ny : dm.nz;
     int a1 = min(a0 + seg, na);
-    bool valid = i < dm.nx;
+    bool valid = i < dm.nx && o < nother;
     T smax = T(0);
     if (valid) {
         int stride = (D == 1) ? dm.nx : dm.nx * dm.ny;
@@ -572,8 +581,8 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(Batc
     const T* __restrict__ F = (const T*)rp.F;
     T* __restrict__ E = (T*)rp.E;
     int i, j, k0, k1;
-    decode_cellz<ONE>(local, dm, i, j, k0, k1);
-    if (i >= dm.nx) return;
+    decode_cellz<ONE>(local, dm, rp.tws, i, j, k0, k1);
+    if (i >= dm.nx || j >= dm.ny) return;
     const int n = dm.n;
     const int plane = dm.nx * dm.ny;
     const int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny);
@@ -715,8 +724,8 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArg
     unsigned long long* floor_hits = &sc->floor_hits;
     unsigned int* status = &sc->status;
     int i, j, k0, k1;
-    decode_cellz<ONE>(local, dm, i, j, k0, k1);
-    const bool valid = i < dm.nx;
+    decode_cellz<ONE>(local, dm, rp.tws, i, j, k0, k1);
+    const bool valid = i < dm.nx && j < dm.ny;
     double cmax = 0.0;
     if (valid) {
         const int n = dm.n;
@@ -742,7 +751,7 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArg
             Ey_xmzm = Ey[cxmzm];
             bzm = ct_bz(S0, E, n, dtdx, czm, cxmzm, cymzm);
         }
-#pragma unroll 2
+#pragma unroll 1
         for (int k = k0; k < k1; ++k) {
             const int c = r0 + k * plane, cxm = rxm + k * plane, cym = rym + k * plane, cxmym = rxmym + k * plane;
             T out[4], Fz0[4];
@@ -829,8 +838,8 @@ __global__ void __launch_bounds__(kBX) k_passive_pred(BatchArgs ba) {
     T* __restrict__ SH = (T*)rp.SH;
     const double dx = rp.dx;
     int i, j, k0, k1;
-    decode_cellz<ONE>(local, dm, i, j, k0, k1);
-    if (i >= dm.nx) return;
+    decode_cellz<ONE>(local, dm, rp.tws, i, j, k0, k1);
+    if (i >= dm.nx || j >= dm.ny) return;
     const int n = dm.n;
     const int plane = dm.nx * dm.ny;
     const T dtdx = (T)(0.5 * sc->dt / dx);
@@ -912,8 +921,8 @@ __global__ void __launch_bounds__(kBX) k_passive_corr(BatchArgs ba) {
     const T* __restrict__ mbnd = (const T*)rp.mbnd;
     const int plane_stride = rp.plane_stride;
     int i, j, k0, k1;
-    decode_cellz<ONE>(local, dm, i, j, k0, k1);
-    if (i >= dm.nx) return;
+    decode_cellz<ONE>(local, dm, rp.tws, i, j, k0, k1);
+    if (i >= dm.nx || j >= dm.ny) return;
     const int n = dm.n;
     const int plane = dm.nx * dm.ny;
     const T dtdx = (T)(sc->dt / dx);
@@ -1104,8 +1113,8 @@ __global__ void __launch_bounds__(kBX) k_force_kick(BatchArgs ba) {
     const int save_bnd = rp.npass > 0;
     const T asqr = (T)(rp.cs * rp.cs);
     int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
-    bool valid = i < dm.nx;
+    decode_cell<ONE>(local, dm, rp.tws, i, j, k);
+    bool valid = i < dm.nx && j < dm.ny;
     const bool inz = k >= rp.zlo && k < rp.zhi;
     double dvmax = 0.0, cmax = 0.0;
     if (valid) {
@@ -1236,9 +1245,9 @@ __global__ void __launch_bounds__(kBX) k_cfl(BatchArgs ba) {
     const T asqr = (T)(rp.cs * rp.cs);
     unsigned long long* out_slots = sc->cfl_slots;
     int i, j, k;
-    decode_cell<ONE>(local, dm, i, j, k);
+    decode_cell<ONE>(local, dm, rp.tws, i, j, k);
     double cm = 0.0;
-    if (i < dm.nx && k >= rp.zlo && k < rp.zhi) {
+    if (i < dm.nx && j < dm.ny && k >= rp.zlo && k < rp.zhi) {
         const int n = dm.n;
         int c = i + dm.nx * (j + dm.ny * k);
         cm = (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],

@@ -44,16 +44,18 @@ static dim3 grid_of(const BatchDev& b, int kind) {
         return dim3((unsigned)b.totals[kind]);
     } else {
         const BoxRec& r = b.a.one;
-        unsigned nbx = (unsigned)((r.nx + kBX - 1) / kBX);
-        if (kind == kKindCell) return dim3(nbx, r.ny, r.nz);
-        if (kind == kKindCellZ) return dim3(nbx, r.ny, (unsigned)((r.nz + kSegZ - 1) / kSegZ));
+        const int tw = 1 << r.tws, th = kBX >> r.tws;
+        unsigned nbx = (unsigned)((r.nx + tw - 1) / tw), nby = (unsigned)((r.ny + th - 1) / th);
+        unsigned nbz = (unsigned)((r.nz + th - 1) / th);
+        if (kind == kKindCell) return dim3(nbx, nby, r.nz);
+        if (kind == kKindCellZ) return dim3(nbx, nby, (unsigned)((r.nz + kSegZ - 1) / kSegZ));
         if (kind == kKindRed) return dim3((unsigned)r.nred);
         switch ((kind - kKindSolver0) % 5) {
-            case kSubCell: return dim3(nbx, r.ny, r.nz);
+            case kSubCell: return dim3(nbx, nby, r.nz);
             case kSubXRow: return dim3(r.ny, r.nz);
             case kSubXTile: return dim3((unsigned)((r.nx + kTX - 1) / kTX), r.ny, r.nz);
-            case kSubMarchY: return dim3(nbx, r.nz, (unsigned)((r.ny + kSeg - 1) / kSeg));
-            default: return dim3(nbx, r.ny, (unsigned)((r.nz + kSeg - 1) / kSeg));
+            case kSubMarchY: return dim3(nbx, nbz, (unsigned)((r.ny + kSeg - 1) / kSeg));
+            default: return dim3(nbx, nby, (unsigned)((r.nz + kSeg - 1) / kSeg));
         }
     }
 }

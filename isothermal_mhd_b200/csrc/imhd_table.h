@@ -23,20 +23,21 @@ inline int reduction_blocks(int n) {
 
 // Blocks of box r for decomposition `kind`.
 inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
-    long nbx = ceil_div(r.nx, kBX);
-    if (kind == kKindCell) return nbx * r.ny * r.nz;
-    if (kind == kKindCellZ) return nbx * r.ny * ceil_div(r.nz, kSegZ);
+    const int tw = 1 << r.tws, th = kBX >> r.tws;
+    long nbx = ceil_div(r.nx, tw), nby = ceil_div(r.ny, th), nbz = ceil_div(r.nz, th);
+    if (kind == kKindCell) return nbx * nby * r.nz;
+    if (kind == kKindCellZ) return nbx * nby * ceil_div(r.nz, kSegZ);
     if (kind == kKindRed) return r.nred;
     int scheme = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
     if (scheme_of(r.riemann, r.recon) != scheme) return 0;
     bool row = row_capable(r.nx, esz);
     switch (sub) {
-        case kSubCell: return nbx * r.ny * r.nz;
+        case kSubCell: return nbx * nby * r.nz;
         case kSubXRow: return row ? (long)r.ny * r.nz : 0;
         case kSubXTile: return row ? 0 : (long)ceil_div(r.nx, kTX) * r.ny * r.nz;
-        case kSubMarchY: return nbx * r.nz * ceil_div(r.ny, kSeg);
-        default: return nbx * r.ny * ceil_div(r.nz, kSeg);
+        case kSubMarchY: return nbx * nbz * ceil_div(r.ny, kSeg);   // (x, z) tiles marching along y
+        default: return nbx * nby * ceil_div(r.nz, kSeg);           // (x, y) tiles marching along z
     }
 }
 
@@ -158,6 +159,9 @@ inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, 
     r.recon = recon;
     r.zlo = 0;
     r.zhi = nz;
+    // widest x tile that the row length divides (whole 128-byte segments per
+    // warp, no idle threads), 32 when none does
+    r.tws = (nx % 128 == 0) ? 7 : (nx % 64 == 0) ? 6 : 5;
     int pmax = ny * nz;
     if (nx * nz > pmax) pmax = nx * nz;
     if (nx * ny > pmax) pmax = nx * ny;

@@ -10,7 +10,7 @@ namespace imhd {
 
 constexpr int kMaxPass = 8;
 constexpr int kSlots = 64;     // spread of the max reductions over addresses
-constexpr int kBX = 128;       // threads along x of the per-cell kernels
+constexpr int kBX = 128;       // threads of the per-cell kernels, as a (1 << tws) x (kBX >> tws) tile
 constexpr int kTX = 128;       // faces per block of the tiled x sweep
 constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
 constexpr int kSegZ = 16;      // cells per thread of the z-marching cell kernels
@@ -27,10 +27,10 @@ enum Stage {
 // Block-decomposition kinds: every launch covers the blocks of all boxes of a
 // table, laid end to end; prefix[kind][b] is the first block of box b.
 enum Kind {
-    kKindCell = 0,     // ceil(nx/kBX) * ny * nz blocks of kBX threads, one cell per thread
+    kKindCell = 0,     // (x, y) tiles of kBX threads per z plane, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
     kKindSolver0 = 2,  // + 5*(scheme-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
-    kKindCellZ = 32,   // ceil(nx/kBX) * ny * ceil(nz/kSegZ) blocks of kBX threads, a z column of kSegZ cells per thread
+    kKindCellZ = 32,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
     kKinds = 33
 };
 // A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
@@ -77,7 +77,7 @@ struct BoxRec {
     int npass, riemann, plane_stride, nred;
     int active, recon;      // running flag; 0 PLM, 1 PPM
     int zlo, zhi;           // z planes whose cells and faces enter the step's maxima and sums
-    int pad2_[2];
+    int tws, pad2_;         // x width of the cell tiles is 1 << tws (32, 64 or 128), height kBX >> tws
     double dx, cs, cour, edot, dt_turb;
     void* S[2];
     void* F;        // 18 flux fields
