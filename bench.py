@@ -38,6 +38,14 @@ WORKLOAD = ("driven MHD turbulence 512^3 periodic box, FP32 van Leer + PLM-char 
             "2 passive scalars, Mach 2 OU forcing, B0=(0.5,0,0), COUR 0.4")
 
 
+def workload_name(a):
+    if (a.n, a.riemann, a.recon, a.npass, a.mach, a.b0x, a.precision) == (512, "roe", "plm", 2, 2.0, 0.5, 32):
+        return WORKLOAD
+    return ("driven MHD turbulence %d^3 periodic box, FP%d van Leer + %s-char + %s + CT, %d passive scalars, "
+            "Mach %g OU forcing, B0=(%g,0,0), COUR %g" % (a.n, a.precision, a.recon.upper(), a.riemann.upper(),
+                                                           a.npass, a.mach, a.b0x, a.cour))
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -50,6 +58,7 @@ def parse():
     ap.add_argument("--precision", type=int, default=32)
     ap.add_argument("--npass", type=int, default=2)
     ap.add_argument("--mach", type=float, default=2.0)
+    ap.add_argument("--b0x", type=float, default=0.5, help="uniform field B0 = (b0x, 0, 0)")
     ap.add_argument("--edot", type=float, default=4.0)
     ap.add_argument("--cour", type=float, default=0.4)
     ap.add_argument("--no-e2e", action="store_true")
@@ -64,6 +73,9 @@ def parse():
                     help="requests of the Poisson stream through the serving loop (0: skip)")
     ap.add_argument("--rate", type=float, default=200.0, help="mean arrival rate of the stream, requests/s")
     ap.add_argument("--hbm-budget", type=float, default=150e9)
+    ap.add_argument("--accuracy", type=int, default=0,
+                    help="instead of timing: run the workload this many steps in FP64 and in FP32 (same dt "
+                         "sequence) and print relative L1 / Linf per field and max |div B|")
     ap.add_argument("--loop-sample", type=int, default=128,
                     help="boxes of the per-box loop arms, the first of the batch (0: all)")
     return ap.parse_args()
@@ -143,10 +155,10 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- workload
-def make_initial_state(n, mach, npass, seed):
+def make_initial_state(n, mach, npass, seed, b0x=0.5):
     from isothermal_mhd_b200 import forcing
     f = forcing.OUForcing(n, seed=seed)
-    q, b, p = forcing.turbulent_box(n, mach=mach, b0=(0.5, 0.0, 0.0), npass=npass, seed=seed, forcing=f)
+    q, b, p = forcing.turbulent_box(n, mach=mach, b0=(b0x, 0.0, 0.0), npass=npass, seed=seed, forcing=f)
     f.advance(0.05)
     delv = f.field(rms=1.0)
     return q, b, p, delv, f
@@ -175,7 +187,7 @@ def run_ours(a, ws, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = a.n
-    q, b, p, delv, f = make_initial_state(n, a.mach, a.npass, a.seed + rank)
+    q, b, p, delv, f = make_initial_state(n, a.mach, a.npass, a.seed + rank, a.b0x)
     box = Box(n, precision=a.precision, riemann=a.riemann, recon=a.recon, npass=a.npass, cour=a.cour, edot=a.edot,
               dt_turb=0.05, device=local)
     stream = torch.cuda.current_stream(dev)
@@ -316,7 +328,7 @@ def run_ours(a, ws, rank, local):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": t_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if a.precision == 32 else "f64", "data": "synthetic (seeded OU turbulence)",
-        "config": {"workload": WORKLOAD, "n": n, "precision": a.precision, "riemann": a.riemann,
+        "config": {"workload": workload_name(a), "n": n, "precision": a.precision, "riemann": a.riemann,
                    "recon": a.recon + "-char", "npass": a.npass, "mach": a.mach, "edot": a.edot, "cour": a.cour,
                    "parallelism": f"replicas x{ws}", "l2": "inputs larger than L2 (state %.1f GB)" %
                    ((10 + a.npass) * cells * esz / 1e9), "drive_steps_timed": state["drives"] - drives0},
@@ -537,6 +549,74 @@ def run_served(a, local):
     return out
 
 
+# ----------------------------------------------------------------- FP32 vs FP64
+def run_accuracy(a, local):
+    """The bench workload (or --n / --riemann / --recon / --npass variants)
+    advanced `a.accuracy` steps in FP64 on the reference driver schedule, then
+    in FP32 with the FP64 run's dt and drive sequence; relative L1 and Linf
+    of every field of the FP32 state against the FP64 one, and max |div B|
+    (face differences per cell) of both."""
+    import torch
+    from isothermal_mhd_b200 import Box
+
+    n = a.n
+    q, b, p, delv, f = make_initial_state(n, a.mach, a.npass, a.seed, a.b0x)
+
+    def run(prec, plan=None):
+        box = Box(n, precision=prec, riemann=a.riemann, recon=a.recon, npass=a.npass, cour=a.cour, edot=a.edot,
+                  dt_turb=0.05, device=local)
+        box.upload(q, b, p)
+        box.set_force(delv)
+        t, dt, t_turb, rec = 0.0, 1e-15, 0.05, []
+        t0 = time.perf_counter()
+        for s in range(a.accuracy):
+            if plan is None:
+                drive = (t_turb > t) and (t_turb <= t + dt)
+                if drive:
+                    t_turb = max(t_turb + 0.05, t + 1e-2 * dt)
+                    dt = 0.5 * dt
+            else:
+                dt, drive = plan[s]
+            rec.append((dt, drive))
+            dt_new = box.step(dt, drive)
+            t += dt
+            dt = dt_new
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        out = box.download()
+        st = box.status()
+        box.close()
+        return out, rec, el, st
+
+    (q64, b64, p64), plan, el64, st64 = run(64)
+    (q32, b32, p32), _, el32, st32 = run(32, plan)
+    names = ["rho", "mx", "my", "mz", "bx_cc", "by_cc", "bz_cc"]
+    fields = {}
+    for k in range(7):
+        fields[names[k]] = (q32[k], q64[k])
+    for k, nm in enumerate(("bx_face", "by_face", "bz_face")):
+        fields[nm] = (b32[k], b64[k])
+    for k in range(a.npass):
+        fields["pass%d" % k] = (p32[k], p64[k])
+    err = {}
+    for nm, (u, v) in fields.items():
+        d = np.abs(u - v)
+        den = float(np.sum(np.abs(v)))
+        err[nm] = {"rel_l1": float(np.sum(d) / den) if den > 0 else float(np.sum(d)),
+                   "rel_linf": float(np.max(d) / np.max(np.abs(v))) if np.max(np.abs(v)) > 0 else float(np.max(d))}
+
+    def max_div(bf):
+        d = (bf[0] - np.roll(bf[0], 1, axis=2)) + (bf[1] - np.roll(bf[1], 1, axis=1)) + (bf[2] - np.roll(bf[2], 1, axis=0))
+        return float(np.max(np.abs(d)))
+
+    return {"metric": "fp32_vs_fp64", "n": n, "steps": a.accuracy, "riemann": a.riemann, "recon": a.recon,
+            "npass": a.npass, "mach": a.mach, "drive_steps": sum(1 for _, dr in plan if dr),
+            "fields": err, "max_rel_l1": max(v["rel_l1"] for v in err.values()),
+            "max_abs_divB": {"fp64": max_div(b64), "fp32": max_div(b32)},
+            "status": {"fp64": st64, "fp32": st32}, "wall_s": {"fp64": el64, "fp32": el32},
+            "note": "FP32 run replays the FP64 run's dt and drive sequence"}
+
+
 # ----------------------------------------------------------------- CPU reference
 def cpu_reference_sample(a, n_sample, steps, warmup):
     """The CPU restatement of the reference (oracle, FP64, all host threads) on
@@ -584,6 +664,8 @@ def main():
     ws, rank, local = dist_env()
     if a.impl == "reference":
         line = run_reference(a, ws, rank)
+    elif a.accuracy > 0:
+        line = run_accuracy(a, local) if rank == 0 else None
     else:
         line = run_ours(a, ws, rank, local)
     if line is not None and rank == 0:
