@@ -261,6 +261,19 @@ int imhd_batch_init_uniform(imhd_batch* batch, int box, double rho, const double
 int imhd_batch_fourier_field(imhd_batch* batch, int box, int target, const int* kvec, const double* amp, int nmodes,
                              double scale);
 int imhd_batch_set_stream(imhd_batch* batch, void* stream);
+/* Online tuning of the batch's decomposition: the first replays of a run try
+ * y/z sweep segments (16, 8, 32 faces per thread) and x tile widths (the
+ * widest that each row length divides, or 32), one real step each, timed
+ * with CUDA events, by coordinate descent; the fastest is kept for the rest
+ * of the batch's life.  Every setting computes the same bits, so tuning
+ * changes timing only: FP64 tunes both; FP32 tunes the tile width only,
+ * because the first slope of a segment is computed by a separate copy of the
+ * code whose FMA contraction may differ from the loop's, so the segment
+ * length could move the last bit.  enable: 1 on (the default), 0 off,
+ * < 0 leaves it; the current setting is returned (tile_policy 0 widest,
+ * 1 always 32; z_column is the fixed z-column length of the cell kernels). */
+int imhd_batch_tuning(imhd_batch* batch, int enable, int* done, int* tile_policy, int* sweep_segment,
+                      int* z_column);
 long long imhd_batch_launch_count(imhd_batch* batch);
 void imhd_batch_destroy(imhd_batch* batch);
 

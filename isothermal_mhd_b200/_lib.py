@@ -29,7 +29,7 @@ EXPORTS = (
     "imhd_server_stats", "imhd_server_stop", "imhd_server_destroy",
     "imhd_write_xyzcube", "imhd_write_state_dump", "imhd_write_cuts", "imhd_write_restart", "imhd_read_restart",
     "imhd_init_turb", "imhd_generate_force", "imhd_turb_seeds", "imhd_get_force",
-    "imhd_set_geometry", "imhd_pack_planes", "imhd_unpack_planes",
+    "imhd_set_geometry", "imhd_pack_planes", "imhd_unpack_planes", "imhd_batch_tuning",
 )
 NSTAGES = 13
 STAGES = ("force_sums", "pred_flux", "pred_emf", "pred_update", "corr_flux_x", "corr_flux_y", "corr_flux_z",
@@ -188,6 +188,8 @@ def lib():
         L.imhd_pack_planes.restype = i
         L.imhd_unpack_planes.argtypes = [vp, i, i, vp]
         L.imhd_unpack_planes.restype = i
+        L.imhd_batch_tuning.argtypes = [vp, i, ip, ip, ip, ip]
+        L.imhd_batch_tuning.restype = i
         _lib = L
     return _lib
 

@@ -116,6 +116,15 @@ class Batch:
                                              kv.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dptr(am), len(kv),
                                              float(scale)))
 
+    def tuning(self, enable=None):
+        """Online decomposition tuning: enable / disable (None leaves it) and
+        the current setting {done, tile_policy, sweep_segment, z_column}."""
+        d, tp, sg, zc = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        e = -1 if enable is None else (1 if enable else 0)
+        check(lib().imhd_batch_tuning(self._h, e, ctypes.byref(d), ctypes.byref(tp), ctypes.byref(sg),
+                                      ctypes.byref(zc)))
+        return {"done": bool(d.value), "tile_policy": tp.value, "sweep_segment": sg.value, "z_column": zc.value}
+
     def set_stream(self, stream_handle):
         check(lib().imhd_batch_set_stream(self._h, ctypes.c_void_p(stream_handle) if stream_handle else None))
 

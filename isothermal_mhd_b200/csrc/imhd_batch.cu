@@ -47,6 +47,17 @@ struct imhd_batch {
     cudaGraphExec_t exec = nullptr;
     bool graph_dirty = true;
     long long graph_kernels = 0;        // kernel launches of one replay
+    size_t table_cap = 0;               // bytes of the device table
+    // online tuning of the decomposition (x tile width policy, y/z sweep
+    // segment, z column length): the first replays of a run time candidate
+    // settings; they are real steps, and every setting computes the same bits
+    bool tune = true;
+    int tune_stage = 0;                 // 0: z column, 1: sweep segment, 2: tile policy, 3: done
+    int tune_idx = 0;
+    int cfg_tile = 0, cfg_segs = imhd::kSegLog, cfg_segzs = imhd::kSegZLog;   // current setting
+    int best_tile = 0, best_segs = imhd::kSegLog, best_segzs = imhd::kSegZLog;
+    float best_ms = 0.f;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
 namespace {
@@ -214,6 +225,7 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         BCK(cudaMemcpyAsync(x->rec[i].sc, &init, sizeof(init), cudaMemcpyHostToDevice, x->st));
     }
     BCK(imhd::upload_table(x->table, x->rec, plan, x->st, x->b.a));
+    x->table_cap = tab;
     x->b.a.use_one = 0;
     x->b.drive_mode = forcing ? 2 : 0;
     *out = x;
@@ -226,6 +238,8 @@ void imhd_batch_destroy(imhd_batch* x) {
     if (x->st) cudaStreamSynchronize(x->st);
     if (x->exec) cudaGraphExecDestroy(x->exec);
     if (x->graph) cudaGraphDestroy(x->graph);
+    if (x->ev0) cudaEventDestroy(x->ev0);
+    if (x->ev1) cudaEventDestroy(x->ev1);
     void* ptrs[] = {x->pool, x->table, x->staging, x->modes_dev, x->amps_dev};
     for (void* q : ptrs)
         if (q) cudaFree(q);
@@ -338,34 +352,161 @@ int imhd_batch_schedule(imhd_batch* x, int box, double t0, double t_end, long lo
     return IMHD_OK;
 }
 
+namespace {
+
+// x tile width of a box under a tile policy: 0 the widest that the row
+// length divides, 1 always 32
+int tile_of(int policy, int nx) {
+    if (policy == 1) return 5;
+    return (nx % 128 == 0) ? 7 : (nx % 64 == 0) ? 6 : 5;
+}
+
+// Re-key the table to a decomposition setting.  The device records carry the
+// current state buffers and running flags, so they are read back, re-keyed
+// and uploaded with new block lists.
+int apply_setting(imhd_batch* x, int tile, int segs, int segzs) {
+    const int nbox = (int)x->rec.size();
+    std::vector<imhd::BoxRec> recs(nbox);
+    BCK(cudaMemcpyAsync(recs.data(), x->table, sizeof(imhd::BoxRec) * nbox, cudaMemcpyDeviceToHost, x->st));
+    BCK(cudaStreamSynchronize(x->st));
+    for (imhd::BoxRec& r : recs) {
+        r.tws = tile_of(tile, r.nx);
+        r.segs = segs;
+        r.segzs = segzs;
+    }
+    imhd::TablePlan plan;
+    imhd::BatchDev nb = x->b;
+    if (!imhd::plan_table(recs, x->esz, nb, plan)) return bfail(IMHD_E_ARG, "batch too large for one launch");
+    if (plan.bytes > x->table_cap) {
+        BCK(cudaStreamSynchronize(x->st));
+        cudaFree(x->table);
+        x->table = nullptr;
+        BCK(cudaMalloc(&x->table, plan.bytes));
+        x->table_cap = plan.bytes;
+    }
+    BCK(imhd::upload_table(x->table, recs, plan, x->st, nb.a));
+    x->b = nb;
+    x->cfg_tile = tile;
+    x->cfg_segs = segs;
+    x->cfg_segzs = segzs;
+    x->graph_dirty = true;
+    return IMHD_OK;
+}
+
+int capture(imhd_batch* x) {
+    if (!x->graph_dirty) return IMHD_OK;
+    BCK(b64(x) ? imhd::prepare_launch<double>(x->b) : imhd::prepare_launch<float>(x->b));
+    if (x->exec) { cudaGraphExecDestroy(x->exec); x->exec = nullptr; }
+    if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
+    BCK(cudaStreamBeginCapture(x->st, cudaStreamCaptureModeThreadLocal));
+    const long long before = x->b.launches;
+    cudaError_t e = b64(x) ? imhd::run_step<double>(x->b, 1) : imhd::run_step<float>(x->b, 1);
+    x->graph_kernels = x->b.launches - before;    // kernels per replay
+    x->b.launches = before;
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(x->st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return bfail(IMHD_E_CUDA, std::string("graph capture of the batch step failed: ") +
+                                      cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    x->graph = g;
+    BCK(cudaGraphInstantiate(&x->exec, x->graph, 0));
+    x->graph_dirty = false;
+    return IMHD_OK;
+}
+
+// Candidate settings by coordinate descent: sweep segment (16, 8, 32), then
+// the tile policy at the best segment.
+bool next_candidate(imhd_batch* x, int& tile, int& segs, int& segzs) {
+    static const int kLogs[3] = {imhd::kSegLog, 3, 5};
+    // In FP32 the first slope / edge / carried value of a column comes from a
+    // separate copy of the code, whose FMA contraction may differ from the
+    // loop's, so the segment lengths would move bits: FP32 tunes the tile
+    // policy only (a pure thread-to-cell mapping).
+    if (!b64(x) && x->tune_stage < 2) {
+        x->tune_stage = 2;
+        x->tune_idx = 0;
+        if (x->best_ms == 0.f) {          // time the default setting first
+            tile = 0; segs = x->best_segs; segzs = x->best_segzs;
+            x->tune_idx = -1;
+            return true;
+        }
+    }
+    while (x->tune_stage < 3) {
+        if (x->tune_stage == 0 && x->tune_idx < 3) {
+            tile = x->best_tile; segzs = x->best_segzs; segs = kLogs[x->tune_idx];
+            return true;
+        }
+        if (x->tune_stage == 1) {          // reserved (z column length: compile-time)
+            x->tune_stage = 2;
+            x->tune_idx = 0;
+            continue;
+        }
+        if (x->tune_stage == 2 && x->tune_idx < 1) {
+            tile = 1; segs = x->best_segs; segzs = x->best_segzs;
+            return true;
+        }
+        x->tune_stage += 1;
+        x->tune_idx = 0;
+    }
+    return false;
+}
+
+}  // namespace
+
 int imhd_batch_run(imhd_batch* x, int replays) {
     if (!x || replays < 0) return bfail(IMHD_E_ARG, "bad argument");
     BCK(cudaSetDevice(x->device));
-    if (x->graph_dirty) {
-        BCK(b64(x) ? imhd::prepare_launch<double>(x->b) : imhd::prepare_launch<float>(x->b));
-        if (x->exec) { cudaGraphExecDestroy(x->exec); x->exec = nullptr; }
-        if (x->graph) { cudaGraphDestroy(x->graph); x->graph = nullptr; }
-        BCK(cudaStreamBeginCapture(x->st, cudaStreamCaptureModeThreadLocal));
-        const long long before = x->b.launches;
-        cudaError_t e = b64(x) ? imhd::run_step<double>(x->b, 1) : imhd::run_step<float>(x->b, 1);
-        x->graph_kernels = x->b.launches - before;    // kernels per replay
-        x->b.launches = before;
-        cudaGraph_t g = nullptr;
-        cudaError_t e2 = cudaStreamEndCapture(x->st, &g);
-        if (e != cudaSuccess || e2 != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return bfail(IMHD_E_CUDA, std::string("graph capture of the batch step failed: ") +
-                                          cudaGetErrorString(e != cudaSuccess ? e : e2));
+    int r = 0, rc;
+    if (x->tune && x->tune_stage < 3 && replays > 0) {
+        if (!x->ev0) {
+            BCK(cudaEventCreate(&x->ev0));
+            BCK(cudaEventCreate(&x->ev1));
         }
-        x->graph = g;
-        BCK(cudaGraphInstantiate(&x->exec, x->graph, 0));
-        x->graph_dirty = false;
+        int tile, segs, segzs;
+        while (r < replays && next_candidate(x, tile, segs, segzs)) {
+            if ((tile != x->cfg_tile || segs != x->cfg_segs || segzs != x->cfg_segzs) &&
+                (rc = apply_setting(x, tile, segs, segzs)))
+                return rc;
+            if ((rc = capture(x))) return rc;
+            BCK(cudaEventRecord(x->ev0, x->st));
+            BCK(cudaGraphLaunch(x->exec, x->st));
+            BCK(cudaEventRecord(x->ev1, x->st));
+            BCK(cudaEventSynchronize(x->ev1));
+            x->b.launches += x->graph_kernels;
+            float ms = 0.f;
+            BCK(cudaEventElapsedTime(&ms, x->ev0, x->ev1));
+            if (x->best_ms == 0.f || ms < x->best_ms) {
+                x->best_ms = ms;
+                x->best_tile = tile;
+                x->best_segs = segs;
+                x->best_segzs = segzs;
+            }
+            x->tune_idx += 1;
+            ++r;
+        }
+        if (x->tune_stage >= 3 &&
+            (x->best_tile != x->cfg_tile || x->best_segs != x->cfg_segs || x->best_segzs != x->cfg_segzs) &&
+            (rc = apply_setting(x, x->best_tile, x->best_segs, x->best_segzs)))
+            return rc;
     }
-    for (int r = 0; r < replays; ++r) {
+    if ((rc = capture(x))) return rc;
+    for (; r < replays; ++r) {
         BCK(cudaGraphLaunch(x->exec, x->st));
         x->b.launches += x->graph_kernels;
     }
     BCK(cudaStreamSynchronize(x->st));
+    return IMHD_OK;
+}
+
+int imhd_batch_tuning(imhd_batch* x, int enable, int* done, int* tile_policy, int* sweep_segment, int* z_column) {
+    if (!x) return bfail(IMHD_E_ARG, "null argument");
+    if (enable >= 0) x->tune = enable != 0;
+    if (done) *done = x->tune_stage >= 3;
+    if (tile_policy) *tile_policy = x->cfg_tile;
+    if (sweep_segment) *sweep_segment = 1 << x->cfg_segs;
+    if (z_column) *z_column = 1 << x->cfg_segzs;
     return IMHD_OK;
 }
 

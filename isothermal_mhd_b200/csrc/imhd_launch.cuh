@@ -48,14 +48,15 @@ static dim3 grid_of(const BatchDev& b, int kind) {
         unsigned nbx = (unsigned)((r.nx + tw - 1) / tw), nby = (unsigned)((r.ny + th - 1) / th);
         unsigned nbz = (unsigned)((r.nz + th - 1) / th);
         if (kind == kKindCell) return dim3(nbx, nby, r.nz);
-        if (kind == kKindCellZ) return dim3(nbx, nby, (unsigned)((r.nz + kSegZ - 1) / kSegZ));
+        const int sz = 1 << r.segzs, sg = 1 << r.segs;
+        if (kind == kKindCellZ) return dim3(nbx, nby, (unsigned)((r.nz + sz - 1) / sz));
         if (kind == kKindRed) return dim3((unsigned)r.nred);
         switch ((kind - kKindSolver0) % 5) {
             case kSubCell: return dim3(nbx, nby, r.nz);
             case kSubXRow: return dim3(r.ny, r.nz);
             case kSubXTile: return dim3((unsigned)((r.nx + kTX - 1) / kTX), r.ny, r.nz);
-            case kSubMarchY: return dim3(nbx, nbz, (unsigned)((r.ny + kSeg - 1) / kSeg));
-            default: return dim3(nbx, nby, (unsigned)((r.nz + kSeg - 1) / kSeg));
+            case kSubMarchY: return dim3(nbx, nbz, (unsigned)((r.ny + sg - 1) / sg));
+            default: return dim3(nbx, nby, (unsigned)((r.nz + sg - 1) / sg));
         }
     }
 }

@@ -144,9 +144,6 @@ struct Worker {
     double* clocks_dev = nullptr;
     double* clocks_host = nullptr;   // pinned
     size_t clocks_cap = 0;
-    double* dstage = nullptr;        // device doubles, one field of the largest box
-    double* hstage = nullptr;        // pinned, same size
-    size_t stage_cap = 0;
     int* modes_dev = nullptr;
     double* amps_dev = nullptr;
     size_t modes_cap = 0;
@@ -173,26 +170,12 @@ struct Worker {
         for (Resident& r : live)
             if (r.mem) cudaFree(r.mem);
         live.clear();
-        void* p[] = {table, clocks_dev, dstage, modes_dev, amps_dev};
+        void* p[] = {table, clocks_dev, modes_dev, amps_dev};
         for (void* q : p)
             if (q) cudaFree(q);
         if (clocks_host) cudaFreeHost(clocks_host);
-        if (hstage) cudaFreeHost(hstage);
         if (st) cudaStreamDestroy(st);
         st = nullptr;
-    }
-
-    bool ensure_stage(size_t n) {
-        if (n <= stage_cap) return true;
-        if (dstage) cudaFree(dstage);
-        if (hstage) cudaFreeHost(hstage);
-        dstage = nullptr;
-        hstage = nullptr;
-        stage_cap = 0;
-        if (!ck(cudaMalloc((void**)&dstage, n * 8), "staging allocation")) return false;
-        if (!ck(cudaMallocHost((void**)&hstage, n * 8), "pinned staging allocation")) return false;
-        stage_cap = n;
-        return true;
     }
 
     bool ensure_modes(size_t m) {

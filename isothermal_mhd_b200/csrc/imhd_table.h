@@ -26,7 +26,7 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
     const int tw = 1 << r.tws, th = kBX >> r.tws;
     long nbx = ceil_div(r.nx, tw), nby = ceil_div(r.ny, th), nbz = ceil_div(r.nz, th);
     if (kind == kKindCell) return nbx * nby * r.nz;
-    if (kind == kKindCellZ) return nbx * nby * ceil_div(r.nz, kSegZ);
+    if (kind == kKindCellZ) return nbx * nby * ceil_div(r.nz, 1 << r.segzs);
     if (kind == kKindRed) return r.nred;
     int scheme = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
@@ -36,8 +36,8 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
         case kSubCell: return nbx * nby * r.nz;
         case kSubXRow: return row ? (long)r.ny * r.nz : 0;
         case kSubXTile: return row ? 0 : (long)ceil_div(r.nx, kTX) * r.ny * r.nz;
-        case kSubMarchY: return nbx * nbz * ceil_div(r.ny, kSeg);   // (x, z) tiles marching along y
-        default: return nbx * nby * ceil_div(r.nz, kSeg);           // (x, y) tiles marching along z
+        case kSubMarchY: return nbx * nbz * ceil_div(r.ny, 1 << r.segs);   // (x, z) tiles marching along y
+        default: return nbx * nby * ceil_div(r.nz, 1 << r.segs);           // (x, y) tiles marching along z
     }
 }
 
@@ -162,6 +162,8 @@ inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, 
     // widest x tile that the row length divides (whole 128-byte segments per
     // warp, no idle threads), 32 when none does
     r.tws = (nx % 128 == 0) ? 7 : (nx % 64 == 0) ? 6 : 5;
+    r.segs = kSegLog;
+    r.segzs = kSegZLog;
     int pmax = ny * nz;
     if (nx * nz > pmax) pmax = nx * nz;
     if (nx * ny > pmax) pmax = nx * ny;

@@ -12,8 +12,9 @@ constexpr int kMaxPass = 8;
 constexpr int kSlots = 64;     // spread of the max reductions over addresses
 constexpr int kBX = 128;       // threads of the per-cell kernels, as a (1 << tws) x (kBX >> tws) tile
 constexpr int kTX = 128;       // faces per block of the tiled x sweep
-constexpr int kSeg = 16;       // faces per thread of the y / z sweeps
-constexpr int kSegZ = 16;      // cells per thread of the z-marching cell kernels
+constexpr int kSegLog = 4;     // default faces per thread of the y / z sweeps: 1 << kSegLog
+constexpr int kSegZLog = 4;    // cells per thread of the z-marching cell kernels: kSegZ = 1 << kSegZLog
+constexpr int kSegZ = 1 << kSegZLog;
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocksMax = 1024;
 constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
@@ -78,6 +79,7 @@ struct BoxRec {
     int active, recon;      // running flag; 0 PLM, 1 PPM
     int zlo, zhi;           // z planes whose cells and faces enter the step's maxima and sums
     int tws, pad2_;         // x width of the cell tiles is 1 << tws (32, 64 or 128), height kBX >> tws
+    int segs, segzs;        // faces per thread of the y / z sweeps 1 << segs; segzs == kSegZLog (reserved)
     double dx, cs, cour, edot, dt_turb;
     void* S[2];
     void* F;        // 18 flux fields

@@ -122,3 +122,27 @@ def test_init_uniform_equals_uploaded_uniform_state(precision):
     np.testing.assert_array_equal(qb, qg)
     np.testing.assert_array_equal(bb, bg)
     np.testing.assert_array_equal(pb, pg)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_online_tuning_changes_no_bits(precision):
+    # the tuner times eight decomposition settings on the first eight steps;
+    # the result equals the untuned run bit for bit
+    cases = [((32, 24, 40), "roe", 2, "plm"), ((48, 32, 32), "hlld", 0, "ppm"), ((20, 20, 20), "hlle", 1, "plm")]
+    out = []
+    for tune in (True, False):
+        cfgs = [make_config(n, precision=precision, riemann=s, npass=np_, cour=0.4, recon=r) for n, s, np_, r in cases]
+        with Batch(cfgs) as bt:
+            bt.tuning(tune)
+            for i, (n, s, np_, r) in enumerate(cases):
+                ic = problems.smooth_wave_box(n, npass=np_)
+                bt.upload(i, ic[0], ic[1], ic[2] if np_ else None)
+                bt.schedule(i, 12)
+            bt.run(12)
+            st = bt.tuning()
+            assert st["done"] == tune
+            out.append([bt.download(i) for i in range(len(cases))])
+    for a, b in zip(out[0], out[1]):
+        for u, v in zip(a, b):
+            if u is not None:
+                np.testing.assert_array_equal(u, v)
