@@ -99,6 +99,23 @@ def init_dist(ws, backend):
     return dist
 
 
+def max_over_ranks(dist, value, device=None):
+    """Largest `value` over the ranks of the job (the job's time is its
+    slowest rank's); the value itself without a process group."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, ranks, ms_max):
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time."""
+    return units_per_rank * ranks / (ms_max / 1e3)
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
@@ -235,13 +252,9 @@ def run_ours(a, ws, rank, local):
     launches = box.launch_count - launches0
     stages = box.stage_times()
     box.profile(False)
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(dist, ms, dev)
     cells = n ** 3
-    value = cells * a.steps * ws / (t_max / 1e3)
+    value = job_rate(cells * a.steps, ws, t_max)
 
     # ---- end to end through the C ABI with host buffers: pinned host state in,
     # K steps (dt in, dt_next out each step), host state out
@@ -266,11 +279,7 @@ def run_ours(a, ws, rank, local):
         box.download(hq, hb, hp)
         e1.record(stream)
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ems], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(dist, e0.elapsed_time(e1), dev)
         state_bytes = hq.nbytes + hb.nbytes + hp.nbytes
         e2e = {"value": cells * a.steps * ws / (ems / 1e3), "unit": METRIC,
                "h2d_bytes_per_step": int(state_bytes / a.steps + 8),
@@ -304,13 +313,16 @@ def run_ours(a, ws, rank, local):
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": sb[dom] * cells, "ms_per_launch": dom_ms}
 
+    # the batched and served workloads are single-GPU measurements: with
+    # several ranks (replicas of the headline box) they are left out
     batched = served = None
-    if a.batched > 0 or a.served > 0:
+    extras = ws == 1 and (a.batched > 0 or a.served > 0)
+    if extras:
         box.close()
         box = None
-    if a.batched > 0:
+    if extras and a.batched > 0:
         batched = run_batched(a, local, stream, dist, dev)
-    if a.served > 0:
+    if extras and a.served > 0:
         served = run_served(a, local)
 
     cpu = None
