@@ -168,10 +168,35 @@ template <int D> struct Rot {
 // ============================================================ predictor flux
 // First-order interface fluxes (compute_{x,y,z}fluxes_3d with
 // corrector_stage = .FALSE., vanleer_mod.f90:441-478): left/right states are
-// the cell values, the normal field the face value.
-template <class T, int SCHEME, int D, bool ONE>
-__global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
+// the cell values, the normal field the face value.  One kernel computes the
+// three faces x+1/2, y+1/2, z+1/2 of every cell: a thread walks a column of
+// kSegZ cells along z and carries the cell above (its z neighbour) into the
+// next plane, so the cell state is read once for all three sweeps.
+template <class T>
+struct CellQ {
+    T q[10];      // rho, mx, my, mz, Bx_cc, By_cc, Bz_cc, Bx_face, By_face, Bz_face
+};
+template <class T, int NF>
+__device__ __forceinline__ void load_cell(const T* __restrict__ S, int n, int c, CellQ<T>& a) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) a.q[f] = fld(S, f, n)[c];
+}
+// rotated conserved state of sweep D (vanleer_mod.f90:443-461, 605-630,
+// 784-806); the normal field is the face value of the left cell
+template <class T, int D>
+__device__ __forceinline__ void rotated(const CellQ<T>& a, T bn, T* u) {
     using R = Rot<D>;
+    u[0] = a.q[0];
+    u[1] = a.q[R::MN];
+    u[2] = a.q[R::MT1];
+    u[3] = a.q[R::MT2];
+    u[4] = bn;
+    u[5] = a.q[R::BT1];
+    u[6] = a.q[R::BT2];
+}
+
+template <class T, int SCHEME, bool ONE>
+__global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     int local;
     const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubCell), local);
@@ -182,33 +207,56 @@ __global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
     T* __restrict__ F = (T*)rp.F;
     const T cs = (T)rp.cs, asqr = (T)(rp.cs * rp.cs);
     unsigned long long* smax_slots = sc->smax_slots;
-    int i, j, k;
-    decode_cell<ONE>(local, dm, rp.tws, i, j, k);
-    bool valid = i < dm.nx && j < dm.ny;
+    int i, j, k0, k1;
+    decode_cellz<ONE>(local, dm, rp.tws, rp.segzs, i, j, k0, k1);
+    const bool valid = i < dm.nx && j < dm.ny;
     T smax = T(0);
     if (valid) {
-        int c = i + dm.nx * (j + dm.ny * k);
-        int cn;
-        if (D == 0) cn = wrap_up(i, dm.nx) + dm.nx * (j + dm.ny * k);
-        else if (D == 1) cn = i + dm.nx * (wrap_up(j, dm.ny) + dm.ny * k);
-        else cn = i + dm.nx * (j + dm.ny * wrap_up(k, dm.nz));
-        T uL[7], uR[7];
-        uL[0] = fld(S, 0, dm.n)[c]; uL[1] = fld(S, R::MN, dm.n)[c]; uL[2] = fld(S, R::MT1, dm.n)[c];
-        uL[3] = fld(S, R::MT2, dm.n)[c]; uL[4] = fld(S, R::BN, dm.n)[c];
-        uL[5] = fld(S, R::BT1, dm.n)[c]; uL[6] = fld(S, R::BT2, dm.n)[c];
-        uR[0] = fld(S, 0, dm.n)[cn]; uR[1] = fld(S, R::MN, dm.n)[cn]; uR[2] = fld(S, R::MT1, dm.n)[cn];
-        uR[3] = fld(S, R::MT2, dm.n)[cn]; uR[4] = uL[4];
-        uR[5] = fld(S, R::BT1, dm.n)[cn]; uR[6] = fld(S, R::BT2, dm.n)[cn];
-        T Fo[7];
-        T sdrop = T(0);     // faces outside zlo..zhi-1 do not enter smax
-        riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
-        T* Fd = F + (size_t)(6 * D) * dm.n;
-        Fd[c] = Fo[0];
-        Fd[(size_t)dm.n + c] = Fo[1];
-        Fd[2 * (size_t)dm.n + c] = Fo[2];
-        Fd[3 * (size_t)dm.n + c] = Fo[3];
-        Fd[4 * (size_t)dm.n + c] = Fo[5];
-        Fd[5 * (size_t)dm.n + c] = Fo[6];
+        const int n = dm.n;
+        const int plane = dm.nx * dm.ny;
+        const int r0 = i + dm.nx * j;
+        const int rx = wrap_up(i, dm.nx) + dm.nx * j, ry = i + dm.nx * wrap_up(j, dm.ny);
+        CellQ<T> cur;
+        load_cell<T, 10>(S, n, r0 + k0 * plane, cur);
+        for (int k = k0; k < k1; ++k) {
+            const int kp = k * plane;
+            const int c = r0 + kp;
+            CellQ<T> xn, yn, zn;
+            load_cell<T, 7>(S, n, rx + kp, xn);
+            load_cell<T, 7>(S, n, ry + kp, yn);
+            load_cell<T, 10>(S, n, r0 + wrap_up(k, dm.nz) * plane, zn);
+            T sdrop = T(0);     // faces outside zlo..zhi-1 do not enter smax
+            T& sref = (k >= rp.zlo && k < rp.zhi) ? smax : sdrop;
+            T uL[7], uR[7], Fo[7];
+            // x face
+            rotated<T, 0>(cur, cur.q[7], uL);
+            rotated<T, 0>(xn, cur.q[7], uR);
+            riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, sref);
+            {
+                T* Fd = F;
+                Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
+                Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
+            }
+            // y face
+            rotated<T, 1>(cur, cur.q[8], uL);
+            rotated<T, 1>(yn, cur.q[8], uR);
+            riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, sref);
+            {
+                T* Fd = F + (size_t)6 * n;
+                Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
+                Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
+            }
+            // z face
+            rotated<T, 2>(cur, cur.q[9], uL);
+            rotated<T, 2>(zn, cur.q[9], uR);
+            riemann_flux<SOLVER>(uL, uR, cs, asqr, Fo, sref);
+            {
+                T* Fd = F + (size_t)12 * n;
+                Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
+                Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
+            }
+            cur = zn;
+        }
     }
     block_atomic_max<kBX>(smax_slots, (double)smax);
 }

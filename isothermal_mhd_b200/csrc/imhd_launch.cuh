@@ -52,7 +52,7 @@ static dim3 grid_of(const BatchDev& b, int kind) {
         if (kind == kKindCellZ) return dim3(nbx, nby, (unsigned)((r.nz + sz - 1) / sz));
         if (kind == kKindRed) return dim3((unsigned)r.nred);
         switch ((kind - kKindSolver0) % 5) {
-            case kSubCell: return dim3(nbx, nby, r.nz);
+            case kSubCell: return dim3(nbx, nby, (unsigned)((r.nz + kSegZ - 1) / kSegZ));   // z columns
             case kSubXRow: return dim3(r.ny, r.nz);
             case kSubXTile: return dim3((unsigned)((r.nx + kTX - 1) / kTX), r.ny, r.nz);
             case kSubMarchY: return dim3(nbx, nbz, (unsigned)((r.ny + sg - 1) / sg));
@@ -65,10 +65,8 @@ template <class T, int SCHEME, bool ONE>
 static void launch_fluxes_pred(BatchDev& b) {
     if (!b.has_scheme[SCHEME] || b.totals[scheme_kind(SCHEME, kSubCell)] == 0) return;
     dim3 g = grid_of<ONE>(b, scheme_kind(SCHEME, kSubCell));
-    k_pred_flux<T, SCHEME, 0, ONE><<<g, kBX, 0, b.st>>>(b.a);
-    k_pred_flux<T, SCHEME, 1, ONE><<<g, kBX, 0, b.st>>>(b.a);
-    k_pred_flux<T, SCHEME, 2, ONE><<<g, kBX, 0, b.st>>>(b.a);
-    b.launches += 3;
+    k_pred_flux<T, SCHEME, ONE><<<g, kBX, 0, b.st>>>(b.a);
+    b.launches += 1;
 }
 
 // The x-row sweep needs more than 48 KiB of dynamic shared memory for long

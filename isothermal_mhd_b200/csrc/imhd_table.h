@@ -33,7 +33,7 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
     if (scheme_of(r.riemann, r.recon) != scheme) return 0;
     bool row = row_capable(r.nx, esz);
     switch (sub) {
-        case kSubCell: return nbx * nby * r.nz;
+        case kSubCell: return nbx * nby * ceil_div(r.nz, kSegZ);   // z columns of the predictor fluxes
         case kSubXRow: return row ? (long)r.ny * r.nz : 0;
         case kSubXTile: return row ? 0 : (long)ceil_div(r.nx, kTX) * r.ny * r.nz;
         case kSubMarchY: return nbx * nbz * ceil_div(r.ny, 1 << r.segs);   // (x, z) tiles marching along y

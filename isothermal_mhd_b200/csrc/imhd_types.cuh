@@ -30,7 +30,7 @@ enum Stage {
 enum Kind {
     kKindCell = 0,     // (x, y) tiles of kBX threads per z plane, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
-    kKindSolver0 = 2,  // + 5*(scheme-1) + {cell, x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
+    kKindSolver0 = 2,  // + 5*(scheme-1) + {z column (predictor), x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
     kKindCellZ = 32,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
     kKinds = 33
 };
