@@ -42,7 +42,8 @@ def workload_name(a):
     if (a.n, a.riemann, a.recon, a.npass, a.mach, a.b0x, a.precision) == (512, "roe", "plm", 2, 2.0, 0.5, 32):
         return WORKLOAD
     return ("driven MHD turbulence %d^3 periodic box, FP%d van Leer + %s-char + %s + CT, %d passive scalars, "
-            "Mach %g OU forcing, B0=(%g,0,0), COUR %g" % (a.n, a.precision, a.recon.upper(), a.riemann.upper(),
+            "Mach %g OU forcing, B0=(%g,0,0), COUR %g" % (a.n, a.precision, a.recon.upper(),
+                                                           {"roe": "Roe"}.get(a.riemann, a.riemann.upper()),
                                                            a.npass, a.mach, a.b0x, a.cour))
 
 
@@ -184,7 +185,7 @@ def make_initial_state(n, mach, npass, seed, b0x=0.5):
 def stage_bytes(esz, npass):
     """Compulsory HBM bytes per cell of each stage (reads + writes once)."""
     return {
-        "pred_flux": 3 * 13 * esz,        # per sweep: 7 state fields in, 6 fluxes out
+        "pred_flux": 28 * esz,            # 7 state + 3 face fields in; 6 fluxes out per face direction
         "pred_emf": 16 * esz,             # rho, m, B_cc, 6 face EMFs in; 3 corner EMFs out
         "pred_update": 32 * esz,          # 7 state + 12 fluxes + 3 EMFs in; 10 fields out
         "corr_flux_x": 13 * esz, "corr_flux_y": 13 * esz, "corr_flux_z": 13 * esz,
@@ -194,6 +195,14 @@ def stage_bytes(esz, npass):
         "passive_corr": (8 + 3 * npass) * esz,
         "force_sums": 7 * esz, "force_kick": 12 * esz, "finalize": 0,
     }
+
+
+# DRAM bytes per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum over the cells of the
+# launch) from an ncu capture at 256^3 of the same kernel and scheme; traffic grows with the cell count,
+# so a launch at n^3 moves about n^3 times this.  Keyed by (stage, precision, riemann, recon).
+NCU_TRAFFIC_PER_CELL = {
+    ("pred_flux", 32, "roe", "plm"): (677.7e6 + 1157.3e6) / 256 ** 3,
+}
 
 
 def run_ours(a, ws, rank, local):
@@ -308,8 +317,10 @@ def run_ours(a, ws, rank, local):
     dom = max(per_stage, key=lambda k: per_stage[k]["ms_per_launch"])
     dom_ms = per_stage[dom]["ms_per_launch"]
     achieved = sb[dom] * cells / 1e9 / (dom_ms / 1e3)
+    tpc = NCU_TRAFFIC_PER_CELL.get((dom, a.precision, a.riemann, a.recon))
+    traffic = tpc * cells if tpc is not None else None
     roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None,
+                "frac": achieved / hbm_peak, "traffic": traffic,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
                 "algorithmic_bytes_per_launch": sb[dom] * cells, "ms_per_launch": dom_ms}
 

@@ -12,7 +12,11 @@
 //  * the continuity sign flips of the Roe eigenvectors (K98 eq. 2.20) are
 //    dropped: they multiply both a left and the matching right eigenvector,
 //    so they cancel in the dissipation term.
-// Near-degenerate renormalisation constants are still evaluated in FP64.
+//  * the eigenvector renormalisation constants come from forms without
+//    cancellation: cs^2 = a^2 ca^2 / cf^2, the larger of cf^2 - ca^2 and
+//    cf^2 - a^2 as a sum of positive terms and the smaller from their
+//    product cf^2 bt^2.  Only near the triple point (cf^2 - cs^2 small) are
+//    they evaluated in FP64 with the reference's limiting values.
 #pragma once
 
 #include "imhd_physics.cuh"
@@ -37,26 +41,30 @@ __device__ __forceinline__ void flux_roe_fast(const float* uL, const float* uR, 
     float ca2 = qa5 * qa5;
     float bsqr = ca2 + btsqr;
     float tmp1 = asqr + bsqr;
-    float dd = asqr - bsqr;
-    float tmp2 = sqrtf(dd * dd + 4.0f * asqr * btsqr);
-    float cs2 = fmaxf(0.0f, 0.5f * (tmp1 - tmp2));
+    float dac = asqr - ca2;
+    float dd = dac - btsqr;
+    float tmp2 = sqrtf(dd * dd + 4.0f * asqr * btsqr);     // cf^2 - cs^2
     float cf2 = 0.5f * (tmp1 + tmp2);
-    float css = sqrtf(cs2), cf = sqrtf(cf2), ca = fabsf(qa5);
     float icf = rsqrtf(cf2);
+    float ca = fabsf(qa5), cf = cf2 * icf;
+    float css = cs * ca * icf;                             // cf^2 cs^2 = a^2 ca^2
     float ev0 = vx2 - cf, ev1 = vx2 - ca, ev2 = vx2 - css, ev3 = vx2 + css, ev4 = vx2 + ca, ev5 = vx2 + cf;
     smax = fmaxf(smax, fabsf(vx2) + cf);
 
     float af, as;
-    float thr = 1.0e-3f * cf2;
-    if ((cf2 - cs2 < thr) || (fabsf(cf2 - ca2) < thr) || (fabsf(cf2 - asqr) < thr)) {
+    if (tmp2 < 1.0e-2f * cf2) {
         double afd, asd;
         roe_alphas_fp64((double)qa5, (double)qa6, (double)qa7, (double)asqr, afd, asd);
         af = (float)afd;
         as = (float)asd;
     } else {
-        float t = rsqrtf(cf2 - cs2);
-        af = sqrtf(fmaxf(0.0f, cf2 - ca2)) * t;
-        as = sqrtf(fmaxf(0.0f, cf2 - asqr)) * t;
+        // af = sqrt(cf^2 - ca^2) / sqrt(cf^2 - cs^2), as = sqrt(cf^2 - a^2) / sqrt(cf^2 - cs^2): the
+        // larger radicand is big, the smaller cf^2 bt^2 / big
+        float big = 0.5f * (fabsf(dac) + btsqr + tmp2);
+        float q = rsqrtf(big * tmp2);
+        float cfbt = cf * sqrtf(btsqr);
+        af = (dac >= 0.0f ? big : cfbt) * q;
+        as = (dac >= 0.0f ? cfbt : big) * q;
     }
     float gy, gz;
     if (btsqr < 1.0e-30f) {
@@ -291,22 +299,36 @@ __device__ __forceinline__ void plm_char_slope_fast(const float* wm, const float
     float rhos = rho * irhos;
     float bx = irhos * bn, by = irhos * w0[4], bz = irhos * w0[5];
     float btsqr = by * by + bz * bz;
-    float bsqr = bx * bx + btsqr;
-    float tmp1 = asqr + bsqr, dd = asqr - bsqr;
-    float tmp2 = sqrtf(dd * dd + 4.0f * asqr * btsqr);
-    float cs2 = fmaxf(0.0f, 0.5f * (tmp1 - tmp2));
+    float ca2 = bx * bx;
+    float bsqr = ca2 + btsqr;
+    float tmp1 = asqr + bsqr;
+    float dac = asqr - ca2;
+    float dd = dac - btsqr;
+    float tmp2 = sqrtf(dd * dd + 4.0f * asqr * btsqr);     // cf^2 - cs^2
     float cf2 = 0.5f * (tmp1 + tmp2);
-    float css = sqrtf(cs2), cf = sqrtf(cf2);
+    float icf = rsqrtf(cf2);
+    float cf = cf2 * icf;
+    float css = cs * fabsf(bx) * icf;                      // cf^2 cs^2 = a^2 ca^2
     float af, as;
-    if (cf2 - cs2 < 1.0e-3f * cf2) {
+    if (tmp2 < 1.0e-2f * cf2) {
         double afd, asd;
         prim_alphas_fp64<float>((double)rho, (double)bn, (double)w0[4], (double)w0[5], (double)asqr, afd, asd);
         af = (float)afd;
         as = (float)asd;
     } else {
-        float inv = 1.0f / (cf2 - cs2);
-        af = sqrtf(fmaxf((asqr - cs2) * inv, 0.0f));
-        as = sqrtf(fmaxf((cf2 - asqr) * inv, 0.0f));
+        // af^2 = (a^2 - cs^2) / tmp2 = a^2 (cf^2 - ca^2) / (cf^2 tmp2), as^2 = (cf^2 - a^2) / tmp2; the
+        // larger of cf^2 - ca^2 and cf^2 - a^2 is big, the smaller cf^2 bt^2 / big
+        float big = 0.5f * (fabsf(dac) + btsqr + tmp2);
+        float bt = sqrtf(btsqr);
+        if (dac >= 0.0f) {
+            float q = rsqrtf(cf2 * tmp2 * big);
+            af = cs * big * q;
+            as = cf2 * bt * q;
+        } else {
+            float q = rsqrtf(tmp2 * big);
+            af = cs * bt * q;
+            as = big * q;
+        }
     }
     float gy, gz;
     if (btsqr < 1.0e-30f) {
