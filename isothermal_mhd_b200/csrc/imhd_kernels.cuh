@@ -877,9 +877,11 @@ __device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int c
 // first-order upwind fluxes and the step-start velocity (passive_mod.f90:
 // 133-157, 204-224, 562-590).
 // A thread walks a column of kSegZ cells along z, carrying the z-neighbour
-// velocities and scalars of the previous cell.
+// velocities and scalars of the previous cell.  The neighbour loads are
+// latency-bound, so FP32 with up to four scalars runs eight blocks per SM
+// (64 registers).
 template <class T, bool ONE, int NP>
-__global__ void __launch_bounds__(kBX) k_passive_pred(BatchArgs ba) {
+__global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_passive_pred(BatchArgs ba) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     const Scalars* sc = rp.sc;
@@ -957,8 +959,10 @@ __device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict
 
 // A thread walks a column of kSegZ cells along z, carrying the z-neighbour
 // time-averaged velocities, half-step scalars and their minmod slopes.
+// Eight blocks per SM in FP32 with up to four scalars, as k_passive_pred
+// (a few spilled values cost less than the lost occupancy).
 template <class T, bool ONE, int NP>
-__global__ void __launch_bounds__(kBX) k_passive_corr(BatchArgs ba) {
+__global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_passive_corr(BatchArgs ba) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     const Scalars* sc = rp.sc;
