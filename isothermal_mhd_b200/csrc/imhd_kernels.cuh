@@ -195,8 +195,12 @@ __device__ __forceinline__ void rotated(const CellQ<T>& a, T bn, T* u) {
     u[6] = a.q[R::BT2];
 }
 
+// FP32 occupancy, measured at 512^3: five blocks per SM for the Roe solver
+// (96 registers; fewer registers spill more than the extra warps return), six
+// for HLLD and HLLE (80 registers, 3.9 -> 3.7 ms).
 template <class T, int SCHEME, bool ONE>
-__global__ void __launch_bounds__(kBX) k_pred_flux(BatchArgs ba) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? (scheme_solver(SCHEME) == 1 ? 5 : 6) : 1)
+k_pred_flux(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     int local;
     const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubCell), local);
@@ -294,8 +298,10 @@ __device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int 
 // primitive window w(a-1..a+2) and the slopes delw(a), delw(a+1) in
 // registers; PPM keeps w(a..a+3), the slopes delw(a), delw(a+1) and the right
 // edge of cell a.  Loads stay coalesced along x.
+// FP32: six blocks per SM (80 registers, a few spills): the z sweep had run
+// four blocks at 104 registers; 3.4 -> 3.1 ms (Roe, PLM) at 512^3.
 template <class T, int SCHEME, int D, bool ONE>
-__global__ void __launch_bounds__(kBX) k_corr_flux_march(BatchArgs ba) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     constexpr bool PPM = scheme_recon(SCHEME) == 1;
     int local;
@@ -488,8 +494,10 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
 // exactly once (the tiled kernel above recomputes slopes at tile edges and
 // stages a halo).  PPM evaluates the edges of cells i and i+1 per face.
 // Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
+// FP32: four 256-thread blocks per SM (64 registers): 3.8 -> 3.4 ms (Roe,
+// PLM) at 512^3.
 template <class T, int SCHEME, bool ONE>
-__global__ void __launch_bounds__(256) k_corr_flux_xrow(BatchArgs ba) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     constexpr bool PPM = scheme_recon(SCHEME) == 1;
     extern __shared__ __align__(16) unsigned char xrow_smem[];
