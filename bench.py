@@ -201,7 +201,7 @@ def stage_bytes(esz, npass):
 # launch) from an ncu capture at 256^3 of the same kernel and scheme; traffic grows with the cell count,
 # so a launch at n^3 moves about n^3 times this.  Keyed by (stage, precision, riemann, recon).
 NCU_TRAFFIC_PER_CELL = {
-    ("pred_flux", 32, "roe", "plm"): (677.7e6 + 1157.3e6) / 256 ** 3,
+    ("pred_flux", 32, "roe", "plm"): (677.4e6 + 1161.1e6) / 256 ** 3,
 }
 
 

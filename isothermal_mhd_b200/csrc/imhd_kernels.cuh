@@ -767,7 +767,7 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
 // ZR: some box of the table restricts its maxima to a z range (slabs); the
 // other instantiation has no per-plane test on the hot path.
 template <class T, bool ONE, bool ZR>
-__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 5 : 1) k_update(BatchArgs ba, double dt_scale, int final_stage) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArgs ba, double dt_scale, int final_stage) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     Scalars* sc = rp.sc;
