@@ -54,6 +54,7 @@ extern "C" {
 #define IMHD_S_NAN 2u       /* a non-finite max speed was seen */
 #define IMHD_S_ZERO_SPEED 4u/* max speed < 1e-20 (vanleer_mod.f90:3328) */
 #define IMHD_S_FORCE 8u     /* forcing quadratic term <= 1e-20 (turb_driver_mod.f90:420) */
+#define IMHD_S_WAIT 16u     /* a bounded wait for an asynchronous copy in a kernel gave up; the step is not valid */
 
 typedef struct imhd_config {
     int nx, ny, nz;        /* interior cells per axis (constants_mod.f90:9-11) */

@@ -422,6 +422,7 @@ int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
     if ((rc = accumulate_stage_times(x))) return rc;
     if (dt_next) *dt_next = x->hio[1];
     unsigned st = *(unsigned*)(x->hio + 2);
+    if (st & IMHD_S_WAIT) return fail(IMHD_E_CUDA, "a bounded wait for an asynchronous copy gave up");
     if (st & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
     if (st & IMHD_S_FORCE) return fail(IMHD_E_PHYSICS, "bad value in turbulence driver energy normalisation");
     return IMHD_OK;

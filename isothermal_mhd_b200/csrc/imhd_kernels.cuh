@@ -868,6 +868,213 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
     if (do_cfl) block_atomic_max<kBX>(cmax_slots, cmax);
 }
 
+// ------------------------------------------------------------ update, TMA-fed
+// The same update for single boxes whose rows are whole 128-cell tiles: a
+// block owns a 128-cell row segment and walks kSegZ planes; thread 0 streams
+// each plane's operands into shared memory with bulk asynchronous copies
+// (cp.async.bulk, completion counted on an mbarrier), one plane ahead of the
+// plane being computed, so that the loads' latency overlaps the arithmetic
+// without registers held for them.  Per plane: 29 row segments of 128 cells
+// (22 fields of row j, 7 of row j-1) and 8 16-byte segments that end at the
+// cell left of the tile (the periodic image at i = nx-1 for the first tile).
+// Every wait is bounded: on time-out the kernel sets IMHD_S_WAIT in the
+// status word, skips the arithmetic and drains its copies with a bounded
+// wait before it exits.
+constexpr int kTmaTile = 128;
+constexpr int kTmaRows = 29;
+constexpr int kTmaHalos = 8;
+constexpr unsigned kStatusWait = 16u;        // IMHD_S_WAIT
+constexpr long long kTmaSpin = 1ll << 24;   // try_wait polls before a wait gives up
+template <class T>
+constexpr int tma_stage_bytes() { return kTmaRows * kTmaTile * (int)sizeof(T) + kTmaHalos * 16; }
+template <class T>
+constexpr size_t update_tma_smem_bytes() { return 2 * (size_t)tma_stage_bytes<T>(); }
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// true once the phase with the given parity has completed; false after kTmaSpin polls
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned a = smem_addr(bar);
+    for (long long it = 0; it < kTmaSpin; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// global -> shared bulk copy of `bytes` (16-byte aligned ends), completion counted on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template <class T, bool ZR>
+__global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
+    k_update_tma(BatchArgs ba, double dt_scale, int final_stage) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    const BoxRec& rp = ba.one;
+    Scalars* sc = rp.sc;
+    if (!rp.active) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ Sout = (T*)rp.S[1];
+    const T* __restrict__ F = (const T*)rp.F;
+    const T* __restrict__ E = (const T*)rp.E;
+    const T asqr = (T)(rp.cs * rp.cs);
+    const int do_cfl = final_stage && !sc->drive;
+    const int t = (int)threadIdx.x;
+    const int i0 = (int)blockIdx.x * kTmaTile, i = i0 + t, j = (int)blockIdx.y;
+    const int k0 = (int)blockIdx.z * kSegZ, k1 = min(k0 + kSegZ, dm.nz);
+    const int n = dm.n, plane = dm.nx * dm.ny;
+    const int jm = wrap_dn(j, dm.ny);
+    const T dtdx = (T)(dt_scale * sc->dt / rp.dx);
+    constexpr int HE = 16 / (int)sizeof(T);          // elements of a 16-byte segment
+    const int ih = (i0 == 0 ? dm.nx : i0) - HE;       // segment ending at the cell left of the tile
+    if (t == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // operand rows of plane k into stage g
+    auto issue = [&](int g, int k) {
+        unsigned char* st = tma_smem + (size_t)g * tma_stage_bytes<T>();
+        T* rows = (T*)st;
+        unsigned char* halo = st + kTmaRows * kTmaTile * sizeof(T);
+        unsigned long long* bar = &bars[g];
+        mbar_expect_tx(bar, (unsigned)tma_stage_bytes<T>());
+        const size_t rj = (size_t)i0 + (size_t)dm.nx * (j + (size_t)dm.ny * k);
+        const size_t rjm = (size_t)i0 + (size_t)dm.nx * (jm + (size_t)dm.ny * k);
+        const size_t hj = (size_t)ih + (size_t)dm.nx * (j + (size_t)dm.ny * k);
+        const size_t hjm = (size_t)ih + (size_t)dm.nx * (jm + (size_t)dm.ny * k);
+        const unsigned rb = kTmaTile * sizeof(T);
+        auto row = [&](int r, const T* base, size_t ofs) { bulk_g2s(rows + r * kTmaTile, base + ofs, rb, bar); };
+        auto hal = [&](int h, const T* base, size_t ofs) { bulk_g2s(halo + h * 16, base + ofs, 16u, bar); };
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int fy = (v == 0) ? 0 : 1 + (v + 1) % 3, fz = (v == 0) ? 0 : 1 + v % 3;
+            row(v, fld(S0, v, n), rj);
+            row(7 + v, F + (size_t)v * n, rj);
+            row(11 + v, F + (size_t)(6 + fy) * n, rj);
+            row(15 + v, F + (size_t)(12 + fz) * n, rj);
+            row(22 + v, F + (size_t)(6 + fy) * n, rjm);
+            hal(v, F + (size_t)v * n, hj);
+        }
+#pragma unroll
+        for (int f = 0; f < 3; ++f) {
+            row(4 + f, fld(S0, 7 + f, n), rj);
+            row(19 + f, E + (size_t)f * n, rj);
+        }
+        row(26, fld(S0, 8, n), rjm);
+        row(27, E, rjm);
+        row(28, E + 2 * (size_t)n, rjm);
+        hal(4, fld(S0, 7, n), hj);
+        hal(5, E + (size_t)n, hj);
+        hal(6, E + 2 * (size_t)n, hj);
+        hal(7, E + 2 * (size_t)n, hjm);
+    };
+    if (t == 0) issue(0, k0);
+
+    unsigned long long* cmax_slots = sc->cmax_slots;
+    double cmax = 0.0;
+    bool ok = true;
+    // values of plane k-1 (periodic image for the first plane of the segment)
+    const int im = wrap_dn(i, dm.nx);
+    const int r0 = i + dm.nx * j, rxm = im + dm.nx * j, rym = i + dm.nx * jm;
+    T Fzm[4], Ex_zm, Ey_zm, Ex_ymzm, Ey_xmzm, bzm;
+    {
+        const int km = wrap_dn(k0, dm.nz);
+        const int czm = r0 + km * plane, cxmzm = rxm + km * plane, cymzm = rym + km * plane;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
+            Fzm[v] = F[(size_t)(12 + fz) * n + czm];
+        }
+        Ex_zm = E[czm];
+        Ey_zm = E[(size_t)n + czm];
+        Ex_ymzm = E[cymzm];
+        Ey_xmzm = E[(size_t)n + cxmzm];
+        bzm = ct_bz(S0, E, n, dtdx, czm, cxmzm, cymzm);
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int it = k - k0, g = it & 1;
+        if (t == 0 && k + 1 < k1) issue(g ^ 1, k + 1);
+        if (ok && !mbar_wait(&bars[g], (unsigned)((it >> 1) & 1))) {
+            ok = false;
+            atomicOr(&sc->status, kStatusWait);
+        }
+        if (ok) {
+            const T* rows = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>());
+            const T* halo = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>() + kTmaRows * kTmaTile * sizeof(T));
+            auto at = [&](int r) { return rows[r * kTmaTile + t]; };
+            auto xm = [&](int r, int h) { return t > 0 ? rows[r * kTmaTile + t - 1] : halo[h * HE + HE - 1]; };
+            const int c = r0 + k * plane;
+            T out[4], Fz0[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                Fz0[v] = at(15 + v);
+                out[v] = at(v) - dtdx * ((at(7 + v) - xm(7 + v, v)) + (at(11 + v) - at(22 + v)) + (Fz0[v] - Fzm[v]));
+            }
+            const bool inz = !ZR || (k >= rp.zlo && k < rp.zhi);
+            if (out[0] < T(kMIN_DENS)) {
+                out[0] = T(kMIN_DENS);
+                if (inz) atomicAdd(&sc->floor_hits, 1ull);
+            }
+            const T Ex0 = at(19), Ey0 = at(20), Ez0 = at(21);
+            const T Ex_ym = at(27), Ey_xm = xm(20, 5);
+            const T Ez_ym = at(28), Ez_xm = xm(21, 6), Ez_xmym = xm(28, 7);
+            const T bx = at(4) - dtdx * ((Ez0 - Ez_ym) - (Ey0 - Ey_zm));
+            const T by = at(5) - dtdx * ((Ex0 - Ex_zm) - (Ez0 - Ez_xm));
+            const T bz = at(6) - dtdx * ((Ey0 - Ey_xm) - (Ex0 - Ex_ym));
+            const T bxm = xm(4, 4) - dtdx * ((Ez_xm - Ez_xmym) - (Ey_xm - Ey_xmzm));
+            const T bym = at(26) - dtdx * ((Ex_ym - Ex_ymzm) - (Ez_ym - Ez_xmym));
+            const T bxc = T(0.5) * (bx + bxm);
+            const T byc = T(0.5) * (by + bym);
+            const T bzc = T(0.5) * (bz + bzm);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
+            fld(Sout, 4, n)[c] = bxc;
+            fld(Sout, 5, n)[c] = byc;
+            fld(Sout, 6, n)[c] = bzc;
+            fld(Sout, 7, n)[c] = bx;
+            fld(Sout, 8, n)[c] = by;
+            fld(Sout, 9, n)[c] = bz;
+            if (do_cfl && inz)
+                cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
+            if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
+                         isfinite(by) && isfinite(bz)))
+                atomicOr(&sc->status, 2u);
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Fzm[v] = Fz0[v];
+            Ex_zm = Ex0;
+            Ey_zm = Ey0;
+            Ex_ymzm = Ex_ym;
+            Ey_xmzm = Ey_xm;
+            bzm = bz;
+        }
+        __syncthreads();   // every thread is done with stage g before it is refilled
+    }
+    // a wait that gave up may leave copies in flight: let them land (bounded) before exit
+    if (t == 0 && !ok) {
+        const int last = k1 - 1 - k0;
+        mbar_wait(&bars[last & 1], (unsigned)((last >> 1) & 1));
+    }
+    if (do_cfl) block_atomic_max<kTmaTile>(cmax_slots, cmax);
+}
+
 // ============================================================ passive scalars
 // Upwind flux of compute_fluxes_1d (passive_mod.f90:594-627).
 template <class T>

@@ -82,8 +82,44 @@ static void ensure_xrow_attr() {
     }
 }
 
+// The TMA-fed update's two stages exceed 48 KiB of shared memory in FP64.
+template <class T>
+static void ensure_update_tma_attr() {
+    static bool attr_set[64] = {};   // per precision and device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        const int bytes = (int)update_tma_smem_bytes<T>();
+        cudaFuncSetAttribute(k_update_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_update_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+}
+
+// Update of one stage: the TMA-fed kernel for a single box whose rows are
+// whole 128-cell tiles, the z-column kernel otherwise.
+template <class T, bool ONE>
+static void launch_update(BatchDev& b, double dt_scale, int final_stage) {
+    const dim3 gz = grid_of<ONE>(b, kKindCellZ);
+    // the bulk copies need 16-byte aligned sources: every row of a 128-cell
+    // tile starts on one when the field bases do
+    const bool aligned = ((uintptr_t)b.a.one.S[0] | (uintptr_t)b.a.one.F | (uintptr_t)b.a.one.E) % 16 == 0;
+    if (ONE && aligned && b.a.one.nx % kTmaTile == 0 && (1 << b.a.one.tws) == kTmaTile) {
+        ensure_update_tma_attr<T>();
+        const dim3 g((unsigned)(b.a.one.nx / kTmaTile), (unsigned)b.a.one.ny, (unsigned)((b.a.one.nz + kSegZ - 1) / kSegZ));
+        const size_t smem = update_tma_smem_bytes<T>();
+        if (b.any_zrange) k_update_tma<T, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+        else k_update_tma<T, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+    } else {
+        if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
+        else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
+    }
+    b.launches += 1;
+}
+
 template <class T>
 cudaError_t prepare_launch(BatchDev& b) {
+    ensure_update_tma_attr<T>();
     for_schemes([&](auto s) {
         if (b.has_scheme[s.value]) {
             ensure_xrow_attr<T, s.value, true>();
@@ -142,9 +178,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStPredEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
     mark(b, kStPredUpdate);
-    if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
-    else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, 0.5, 0);
-    b.launches += 2;
+    launch_update<T, ONE>(b, 0.5, 0);
+    b.launches += 1;
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
     mark(b, kStCorrFluxX);
@@ -156,9 +191,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStCorrEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
     mark(b, kStFinalUpdate);
-    if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
-    else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, 1.0, 1);
-    b.launches += 2;
+    launch_update<T, ONE>(b, 1.0, 1);
+    b.launches += 1;
     if (b.drive_mode) {
         mark(b, kStForceKick);
         k_force_kick<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);

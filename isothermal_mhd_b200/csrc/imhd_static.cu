@@ -145,6 +145,7 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &rec.sc->status, sizeof(unsigned), cudaMemcpyDeviceToHost, b.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b.st);
     if (e != cudaSuccess) return fail(IMHD_E_CUDA, std::string("imhd_step_static: ") + cudaGetErrorString(e));
+    if (status & IMHD_S_WAIT) return fail(IMHD_E_CUDA, "a bounded wait for an asynchronous copy gave up");
     if (status & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
     if (dt_next) *dt_next = host_io[1];
     return IMHD_OK;

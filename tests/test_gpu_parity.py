@@ -71,6 +71,42 @@ def test_fp64_bit_exact_32_roe():
     assert_exact(g, o)
 
 
+# Rows that are whole 128-cell tiles take the TMA-fed update kernel (bulk
+# copies of each plane's rows into shared memory); nz = 18 and 20 leave a
+# partial last z segment, the row below j = 0 wraps to ny - 1, and the first tile
+# of each row reads its left neighbour from the periodic image at nx - 1.
+@pytest.mark.parametrize("riemann,n", [("roe", (128, 12, 20)), ("hlld", (256, 12, 18)), ("hlle", (256, 12, 18))])
+def test_fp64_bit_exact_tma_update_rows(riemann, n):
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, riemann, steps=4, nthreads=8)
+    g = gpu_run(ic, n, riemann, steps=4)
+    assert_exact(g, o)
+
+
+def test_fp64_tma_update_rows_driven():
+    from oracle.pyoracle import Oracle
+    n = (128, 12, 18)
+    ic = problems.smooth_wave_box(n, npass=1)
+    gen = Oracle(n, riemann="roe", npass=1)
+    delv = gen.generate_ref_force(seeds=(1234, 5678, 9123))
+    gen.close()
+    o = oracle_run(ic, n, "roe", steps=4, force=delv, drive_at=(1,), edot=1.0, nthreads=8)
+    g = gpu_run(ic, n, "roe", steps=4, force=delv, drive_at=(1,), edot=1.0, dts=o["dts"])
+    for name in ("q", "b", "p"):
+        err = rel_l1(g[name], o[name])
+        assert np.all(err <= 1e-12), (name, err)
+
+
+def test_fp32_tma_update_rows_within_1e5():
+    n = (256, 12, 18)
+    ic = problems.smooth_wave_box(n, npass=1)
+    o = oracle_run(ic, n, "roe", steps=10, nthreads=8)
+    g = gpu_run(ic, n, "roe", steps=10, precision=32, dts=o["dts"])
+    for name in ("q", "b", "p"):
+        err = rel_l1(g[name], o[name])
+        assert np.all(err <= 1e-5), (name, err)
+
+
 @pytest.mark.parametrize("riemann", SOLVERS)
 def test_fp64_bit_exact_ppm_noncubic(riemann):
     # PPM characteristic reconstruction (the reference default) on all sweeps
