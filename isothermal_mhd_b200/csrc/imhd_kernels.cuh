@@ -876,7 +876,9 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
 // plane being computed, so that the loads' latency overlaps the arithmetic
 // without registers held for them.  Per plane: 29 row segments of 128 cells
 // (22 fields of row j, 7 of row j-1) and 8 16-byte segments that end at the
-// cell left of the tile (the periodic image at i = nx-1 for the first tile).
+// cell left of the tile (the periodic image at i = nx-1 for the first tile),
+// each stored just in front of its row so that the left neighbour of every
+// cell is the element before it.  Lane r of warp 0 issues row r.
 // Every wait is bounded: on time-out the kernel sets IMHD_S_WAIT in the
 // status word, skips the arithmetic and drains its copies with a bounded
 // wait before it exits.
@@ -886,7 +888,11 @@ constexpr int kTmaHalos = 8;
 constexpr unsigned kStatusWait = 16u;        // IMHD_S_WAIT
 constexpr long long kTmaSpin = 1ll << 24;   // try_wait polls before a wait gives up
 template <class T>
-constexpr int tma_stage_bytes() { return kTmaRows * kTmaTile * (int)sizeof(T) + kTmaHalos * 16; }
+constexpr int tma_row_stride() { return kTmaTile + 16 / (int)sizeof(T); }   // a 16-byte halo slot + the row
+template <class T>
+constexpr int tma_copy_bytes() { return kTmaRows * kTmaTile * (int)sizeof(T) + kTmaHalos * 16; }
+template <class T>
+constexpr int tma_stage_bytes() { return (kTmaRows * tma_row_stride<T>() * (int)sizeof(T) + 127) / 128 * 128; }
 template <class T>
 constexpr size_t update_tma_smem_bytes() { return 2 * (size_t)tma_stage_bytes<T>(); }
 
@@ -949,44 +955,35 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
         mbar_init_fence();
     }
     __syncthreads();
-    // operand rows of plane k into stage g
+    // operand rows of plane k into stage g: row r (and its halo) by lane r of warp 0
+    constexpr int RS = tma_row_stride<T>();
     auto issue = [&](int g, int k) {
-        unsigned char* st = tma_smem + (size_t)g * tma_stage_bytes<T>();
-        T* rows = (T*)st;
-        unsigned char* halo = st + kTmaRows * kTmaTile * sizeof(T);
+        T* rows = (T*)(tma_smem + (size_t)g * tma_stage_bytes<T>());
         unsigned long long* bar = &bars[g];
-        mbar_expect_tx(bar, (unsigned)tma_stage_bytes<T>());
-        const size_t rj = (size_t)i0 + (size_t)dm.nx * (j + (size_t)dm.ny * k);
-        const size_t rjm = (size_t)i0 + (size_t)dm.nx * (jm + (size_t)dm.ny * k);
-        const size_t hj = (size_t)ih + (size_t)dm.nx * (j + (size_t)dm.ny * k);
-        const size_t hjm = (size_t)ih + (size_t)dm.nx * (jm + (size_t)dm.ny * k);
-        const unsigned rb = kTmaTile * sizeof(T);
-        auto row = [&](int r, const T* base, size_t ofs) { bulk_g2s(rows + r * kTmaTile, base + ofs, rb, bar); };
-        auto hal = [&](int h, const T* base, size_t ofs) { bulk_g2s(halo + h * 16, base + ofs, 16u, bar); };
-#pragma unroll
-        for (int v = 0; v < 4; ++v) {
-            const int fy = (v == 0) ? 0 : 1 + (v + 1) % 3, fz = (v == 0) ? 0 : 1 + v % 3;
-            row(v, fld(S0, v, n), rj);
-            row(7 + v, F + (size_t)v * n, rj);
-            row(11 + v, F + (size_t)(6 + fy) * n, rj);
-            row(15 + v, F + (size_t)(12 + fz) * n, rj);
-            row(22 + v, F + (size_t)(6 + fy) * n, rjm);
-            hal(v, F + (size_t)v * n, hj);
+        if (t == 0) mbar_expect_tx(bar, (unsigned)tma_copy_bytes<T>());
+        __syncwarp();
+        if (t < kTmaRows) {
+            const int r = t;
+            const T* base;
+            int jr = j;
+            if (r < 4) base = fld(S0, r, n);
+            else if (r < 7) base = fld(S0, 3 + r, n);                                        // fields 7-9
+            else if (r < 11) base = F + (size_t)(r - 7) * n;                                  // x fluxes
+            else if (r < 15) base = F + (size_t)(6 + (r == 11 ? 0 : 1 + (r - 11 + 1) % 3)) * n;    // y, by variable
+            else if (r < 19) base = F + (size_t)(12 + (r == 15 ? 0 : 1 + (r - 15) % 3)) * n;       // z, by variable
+            else if (r < 22) base = E + (size_t)(r - 19) * n;
+            else if (r < 26) { base = F + (size_t)(6 + (r == 22 ? 0 : 1 + (r - 22 + 1) % 3)) * n; jr = jm; }
+            else if (r == 26) { base = fld(S0, 8, n); jr = jm; }
+            else if (r == 27) { base = E; jr = jm; }
+            else { base = E + 2 * (size_t)n; jr = jm; }
+            const size_t ofs = (size_t)dm.nx * (jr + (size_t)dm.ny * k);
+            bulk_g2s(rows + r * RS + HE, base + i0 + ofs, kTmaTile * (unsigned)sizeof(T), bar);
+            // rows whose left neighbour is read: x fluxes, bx, Ey, Ez and Ez of row j-1
+            if ((r >= 7 && r <= 10) || r == 4 || r == 20 || r == 21 || r == 28)
+                bulk_g2s(rows + r * RS, base + ih + ofs, 16u, bar);
         }
-#pragma unroll
-        for (int f = 0; f < 3; ++f) {
-            row(4 + f, fld(S0, 7 + f, n), rj);
-            row(19 + f, E + (size_t)f * n, rj);
-        }
-        row(26, fld(S0, 8, n), rjm);
-        row(27, E, rjm);
-        row(28, E + 2 * (size_t)n, rjm);
-        hal(4, fld(S0, 7, n), hj);
-        hal(5, E + (size_t)n, hj);
-        hal(6, E + 2 * (size_t)n, hj);
-        hal(7, E + 2 * (size_t)n, hjm);
     };
-    if (t == 0) issue(0, k0);
+    if (t < 32) issue(0, k0);
 
     unsigned long long* cmax_slots = sc->cmax_slots;
     double cmax = 0.0;
@@ -1011,16 +1008,15 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     }
     for (int k = k0; k < k1; ++k) {
         const int it = k - k0, g = it & 1;
-        if (t == 0 && k + 1 < k1) issue(g ^ 1, k + 1);
+        if (t < 32 && k + 1 < k1) issue(g ^ 1, k + 1);
         if (ok && !mbar_wait(&bars[g], (unsigned)((it >> 1) & 1))) {
             ok = false;
             atomicOr(&sc->status, kStatusWait);
         }
         if (ok) {
-            const T* rows = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>());
-            const T* halo = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>() + kTmaRows * kTmaTile * sizeof(T));
-            auto at = [&](int r) { return rows[r * kTmaTile + t]; };
-            auto xm = [&](int r, int h) { return t > 0 ? rows[r * kTmaTile + t - 1] : halo[h * HE + HE - 1]; };
+            const T* rows = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>()) + HE + t;
+            auto at = [&](int r) { return rows[r * RS]; };
+            auto xm = [&](int r, int) { return rows[r * RS - 1]; };
             const int c = r0 + k * plane;
             T out[4], Fz0[4];
 #pragma unroll
