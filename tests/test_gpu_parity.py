@@ -71,13 +71,20 @@ def test_fp64_bit_exact_32_roe():
     assert_exact(g, o)
 
 
-# Rows that are whole 128-cell tiles take the TMA-fed update kernel (bulk
-# copies of each plane's rows into shared memory); nz = 18 and 20 leave a
-# partial last z segment, the row below j = 0 wraps to ny - 1, and the first tile
-# of each row reads its left neighbour from the periodic image at nx - 1.
-@pytest.mark.parametrize("riemann,n", [("roe", (128, 12, 20)), ("hlld", (256, 12, 18)), ("hlle", (256, 12, 18))])
-def test_fp64_bit_exact_tma_update_rows(riemann, n):
-    ic = problems.smooth_wave_box(n, npass=1)
+# Rows that are whole 128-cell tiles take the TMA-fed update and passive
+# predictor kernels (bulk copies of each plane's rows into shared memory);
+# nz = 18 and 20 leave a partial last z segment, the rows next to j = 0 and
+# j = ny - 1 wrap, and the first and last tiles of each row read their x
+# neighbours from the periodic images.
+@pytest.mark.parametrize("riemann,n,npass", [("roe", (128, 12, 20), 1), ("hlld", (256, 12, 18), 2),
+                                             ("hlle", (256, 12, 18), 4), ("roe", (128, 12, 18), 0)])
+def test_fp64_bit_exact_tma_update_rows(riemann, n, npass):
+    ic = problems.smooth_wave_box(n, npass=max(npass, 1))
+    if npass == 0:
+        ic = (ic[0], ic[1], ic[2][:0])
+    elif npass > 1:
+        rng = np.random.default_rng(7)
+        ic = (ic[0], ic[1], rng.uniform(0.0, 1.0, (npass,) + ic[2].shape[1:]))
     o = oracle_run(ic, n, riemann, steps=4, nthreads=8)
     g = gpu_run(ic, n, riemann, steps=4)
     assert_exact(g, o)
