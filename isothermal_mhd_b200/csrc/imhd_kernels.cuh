@@ -761,6 +761,13 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
     return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
 }
 
+// A table's box goes to the bulk-copy fed update when its rows are whole
+// 128-cell tiles and the bases its copies read from are 16-byte aligned (both
+// update kernels decide from the same record, so exactly one takes the box).
+__device__ __forceinline__ bool update_by_tma(const BoxRec& r) {
+    return r.nx % kTmaTile == 0 && (((uintptr_t)r.S[0] | (uintptr_t)r.F | (uintptr_t)r.E) & 15) == 0;
+}
+
 // A thread walks a column of kSegZ cells along z; the z-face fluxes, the
 // corner EMFs at k and the new face field bz read or computed at plane k are
 // the "k-1" values of plane k+1 and are carried instead of reloaded.
@@ -772,6 +779,7 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     Scalars* sc = rp.sc;
     if (!rp.active) return;
+    if (!ONE && update_by_tma(rp)) return;   // a table's 128k-cell rows go to k_update_tma
     const Dims dm = dims_of(rp);
     const T* __restrict__ S0 = (const T*)rp.S[0];
     T* __restrict__ Sout = (T*)rp.S[1];
@@ -882,7 +890,6 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
 // Every wait is bounded: on time-out the kernel sets IMHD_S_WAIT in the
 // status word, skips the arithmetic and drains its copies with a bounded
 // wait before it exits.
-constexpr int kTmaTile = 128;
 constexpr int kTmaRows = 29;
 constexpr int kTmaHalos = 8;
 constexpr unsigned kStatusWait = 16u;        // IMHD_S_WAIT
@@ -926,14 +933,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  : "memory");
 }
 
-template <class T, bool ZR>
+template <class T, bool ZR, bool ONE>
 __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     k_update_tma(BatchArgs ba, double dt_scale, int final_stage) {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) unsigned long long bars[2];
-    const BoxRec& rp = ba.one;
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindUpdTma, local);
     Scalars* sc = rp.sc;
-    if (!rp.active) return;
+    if (!rp.active || (!ONE && !update_by_tma(rp))) return;
     const Dims dm = dims_of(rp);
     const T* __restrict__ S0 = (const T*)rp.S[0];
     T* __restrict__ Sout = (T*)rp.S[1];
@@ -942,8 +950,19 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     const T asqr = (T)(rp.cs * rp.cs);
     const int do_cfl = final_stage && !sc->drive;
     const int t = (int)threadIdx.x;
-    const int i0 = (int)blockIdx.x * kTmaTile, i = i0 + t, j = (int)blockIdx.y;
-    const int k0 = (int)blockIdx.z * kSegZ, k1 = min(k0 + kSegZ, dm.nz);
+    int i0, j, seg;
+    if constexpr (ONE) {   // grid (nx / 128, ny, z segments)
+        i0 = (int)blockIdx.x * kTmaTile;
+        j = (int)blockIdx.y;
+        seg = (int)blockIdx.z;
+    } else {
+        const int nbx = dm.nx / kTmaTile, rest = local / nbx;
+        i0 = (local % nbx) * kTmaTile;
+        j = rest % dm.ny;
+        seg = rest / dm.ny;
+    }
+    const int i = i0 + t;
+    const int k0 = seg * kSegZ, k1 = min(k0 + kSegZ, dm.nz);
     const int n = dm.n, plane = dm.nx * dm.ny;
     const int jm = wrap_dn(j, dm.ny);
     const T dtdx = (T)(dt_scale * sc->dt / rp.dx);

@@ -90,31 +90,43 @@ static void ensure_update_tma_attr() {
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_set[dev]) {
         const int bytes = (int)update_tma_smem_bytes<T>();
-        cudaFuncSetAttribute(k_update_tma<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(k_update_tma<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_update_tma<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_update_tma<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_update_tma<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        cudaFuncSetAttribute(k_update_tma<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
 }
 
 // Update of one stage: the TMA-fed kernel for a single box whose rows are
-// whole 128-cell tiles, the z-column kernel otherwise.
+// whole 128-cell tiles, the z-column kernel otherwise.  A table launches both:
+// the z-column kernel skips the boxes with such rows (every box of a table is
+// carved on 256-byte boundaries), the TMA-fed kernel covers only those.
 template <class T, bool ONE>
 static void launch_update(BatchDev& b, double dt_scale, int final_stage) {
     const dim3 gz = grid_of<ONE>(b, kKindCellZ);
     // the bulk copies need 16-byte aligned sources: every row of a 128-cell
     // tile starts on one when the field bases do
     const bool aligned = ((uintptr_t)b.a.one.S[0] | (uintptr_t)b.a.one.F | (uintptr_t)b.a.one.E) % 16 == 0;
-    if (ONE && aligned && b.a.one.nx % kTmaTile == 0 && (1 << b.a.one.tws) == kTmaTile) {
+    const size_t smem = update_tma_smem_bytes<T>();
+    if (ONE && aligned && b.a.one.nx % kTmaTile == 0) {
         ensure_update_tma_attr<T>();
         const dim3 g((unsigned)(b.a.one.nx / kTmaTile), (unsigned)b.a.one.ny, (unsigned)((b.a.one.nz + kSegZ - 1) / kSegZ));
-        const size_t smem = update_tma_smem_bytes<T>();
-        if (b.any_zrange) k_update_tma<T, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-        else k_update_tma<T, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-    } else {
-        if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
-        else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
+        if (b.any_zrange) k_update_tma<T, true, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+        else k_update_tma<T, false, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+        b.launches += 1;
+        return;
     }
+    if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
+    else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
     b.launches += 1;
+    if (!ONE && b.totals[kKindUpdTma] > 0) {
+        ensure_update_tma_attr<T>();
+        const unsigned g = (unsigned)b.totals[kKindUpdTma];
+        if (b.any_zrange) k_update_tma<T, true, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+        else k_update_tma<T, false, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+        b.launches += 1;
+    }
 }
 
 template <class T>

@@ -15,6 +15,7 @@ constexpr int kTX = 128;       // faces per block of the tiled x sweep
 constexpr int kSegLog = 4;     // default faces per thread of the y / z sweeps: 1 << kSegLog
 constexpr int kSegZLog = 4;    // cells per thread of the z-marching cell kernels: kSegZ = 1 << kSegZLog
 constexpr int kSegZ = 1 << kSegZLog;
+constexpr int kTmaTile = 128;   // row segment of a block of the bulk-copy fed kernels
 constexpr int kRedThreads = 256;
 constexpr int kRedBlocksMax = 1024;
 constexpr size_t kRowSmemMax = 96 * 1024;   // dynamic shared memory of the x-row sweep
@@ -32,7 +33,8 @@ enum Kind {
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
     kKindSolver0 = 2,  // + 5*(scheme-1) + {z column (predictor), x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
     kKindCellZ = 32,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
-    kKinds = 33
+    kKindUpdTma = 33,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
+    kKinds = 34
 };
 // A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
 // (0 PLM, 1 PPM): scheme = solver + 3 * recon, 1..kSchemes.

@@ -12,8 +12,11 @@ from isothermal_mhd_b200.batch import make_config
 
 pytestmark = pytest.mark.gpu
 
-CASES = [((16, 16, 16), "roe", 1, 6), ((24, 16, 20), "hlld", 2, 4), ((12, 12, 12), "hlle", 0, 8)]
-RECON = ["plm", "ppm", "plm"]      # a PPM box among PLM boxes
+# the 128 x 12 x 18 box has rows of whole 128-cell tiles: its update runs the
+# bulk-copy fed kernel, in the batch (table launch) and alone
+CASES = [((16, 16, 16), "roe", 1, 6), ((24, 16, 20), "hlld", 2, 4), ((12, 12, 12), "hlle", 0, 8),
+         ((128, 12, 18), "roe", 1, 4)]
+RECON = ["plm", "ppm", "plm", "plm"]      # a PPM box among PLM boxes
 
 
 def alone(n, riemann, npass, steps, precision, ic, edot=0.0, delv=None, recon="plm"):
@@ -128,7 +131,8 @@ def test_init_uniform_equals_uploaded_uniform_state(precision):
 def test_online_tuning_changes_no_bits(precision):
     # the tuner times eight decomposition settings on the first eight steps;
     # the result equals the untuned run bit for bit
-    cases = [((32, 24, 40), "roe", 2, "plm"), ((48, 32, 32), "hlld", 0, "ppm"), ((20, 20, 20), "hlle", 1, "plm")]
+    cases = [((32, 24, 40), "roe", 2, "plm"), ((48, 32, 32), "hlld", 0, "ppm"), ((20, 20, 20), "hlle", 1, "plm"),
+             ((128, 12, 16), "roe", 1, "plm")]
     out = []
     for tune in (True, False):
         cfgs = [make_config(n, precision=precision, riemann=s, npass=np_, cour=0.4, recon=r) for n, s, np_, r in cases]
