@@ -100,6 +100,16 @@ int imhd_download(imhd_box* box, double* q, double* bface, double* qpass);
 int imhd_set_force(imhd_box* box, const double* delv);
 /* The force field of the box, in the layout of imhd_set_force. */
 int imhd_get_force(imhd_box* box, double* delv);
+/* This box's forcing sums of its current state over its own planes
+ * (imhd_set_geometry): sums[0] = 1/2 sum rho |delv|^2, sums[1] = sum delv.m,
+ * sums[2..4] = sum rho delv -- get_rho_turb's quad_term1, quad_term2 and
+ * mom{x,y,z}_avg before their all-reduce (turb_driver_mod.f90:158-189).
+ * Needs imhd_set_force. */
+int imhd_force_sums(imhd_box* box, double* sums);
+/* All ranks' sums for the box's next drive step, which then normalises the
+ * kick with them instead of its own (the end_allreduce results of
+ * add_random_force, turb_driver_mod.f90:402-415).  Used once. */
+int imhd_set_force_sums(imhd_box* box, const double* sums);
 
 /* One time step of the reference driver loop for one rank: copy_velocity,
  * vanleer_solve_3d(dt, drive_next) (vanleer_mod.f90:279-426, incl.

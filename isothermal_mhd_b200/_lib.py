@@ -29,6 +29,7 @@ EXPORTS = (
     "imhd_server_stats", "imhd_server_stop", "imhd_server_destroy",
     "imhd_write_xyzcube", "imhd_write_state_dump", "imhd_write_cuts", "imhd_write_restart", "imhd_read_restart",
     "imhd_init_turb", "imhd_generate_force", "imhd_turb_seeds", "imhd_get_force",
+    "imhd_force_sums", "imhd_set_force_sums",
     "imhd_set_geometry", "imhd_pack_planes", "imhd_unpack_planes", "imhd_batch_tuning",
 )
 NSTAGES = 13
@@ -182,6 +183,10 @@ def lib():
         L.imhd_turb_seeds.restype = i
         L.imhd_get_force.argtypes = [vp, dp]
         L.imhd_get_force.restype = i
+        L.imhd_force_sums.argtypes = [vp, dp]
+        L.imhd_force_sums.restype = i
+        L.imhd_set_force_sums.argtypes = [vp, dp]
+        L.imhd_set_force_sums.restype = i
         L.imhd_set_geometry.argtypes = [vp, d, i, i]
         L.imhd_set_geometry.restype = i
         L.imhd_pack_planes.argtypes = [vp, i, i, vp]

@@ -182,6 +182,18 @@ class Box:
     def unpack_planes(self, z0, nplanes, src):
         check(lib().imhd_unpack_planes(self._h, int(z0), int(nplanes), ctypes.c_void_p(src.data_ptr())))
 
+    def force_sums(self):
+        """This box's forcing sums over its own planes (get_rho_turb's five
+        terms before the all-reduce), as a float64 array of 5."""
+        out = np.empty(5)
+        check(lib().imhd_force_sums(self._h, _dptr(out)))
+        return out
+
+    def set_force_sums(self, sums):
+        """All ranks' forcing sums, used by the next drive step's kick."""
+        s = np.ascontiguousarray(np.asarray(sums, dtype=np.float64).reshape(5))
+        check(lib().imhd_set_force_sums(self._h, _dptr(s)))
+
     def get_force(self):
         """The force field (3, nz+2g, ny+2g, nx+2g) in FP64."""
         g = self.cfg.ng

@@ -17,6 +17,7 @@
 namespace imhd {
 template <class T> cudaError_t run_step(BatchDev&, int);
 template <class T> cudaError_t run_max_speed(BatchDev&);
+template <class T> cudaError_t run_force_sums(BatchDev&);
 template <class T> cudaError_t run_diag(BatchDev&);
 template <class T> cudaError_t run_from_f64(cudaStream_t, const double*, void*, int);
 template <class T> cudaError_t run_to_f64(cudaStream_t, const void*, double*, int);
@@ -399,6 +400,30 @@ int imhd_get_force(imhd_box* x, double* delv) {
         ghost_fill(x->cfg, h, x->cfg.ng);
     }
     return IMHD_OK;
+}
+
+int imhd_force_sums(imhd_box* x, double* sums) {
+    if (!x || !sums) return fail(IMHD_E_ARG, "null argument");
+    if (!x->have_force) return fail(IMHD_E_STATE, "imhd_force_sums before imhd_set_force");
+    CK(cudaSetDevice(x->cfg.device));
+    set_one(x);
+    CK(is64(x) ? imhd::run_force_sums<double>(x->b) : imhd::run_force_sums<float>(x->b));
+    CK(cudaMemcpyAsync(x->hio + 24, x->rec.sc->sums, 5 * sizeof(double), cudaMemcpyDeviceToHost, x->b.st));
+    int rc = sync_and_check(x);
+    if (rc) return rc;
+    std::memcpy(sums, x->hio + 24, 5 * sizeof(double));
+    return IMHD_OK;
+}
+
+int imhd_set_force_sums(imhd_box* x, const double* sums) {
+    if (!x || !sums) return fail(IMHD_E_ARG, "null argument");
+    CK(cudaSetDevice(x->cfg.device));
+    std::memcpy(x->hio + 24, sums, 5 * sizeof(double));
+    const unsigned one = 1u;
+    std::memcpy(x->hio + 29, &one, sizeof(one));
+    CK(cudaMemcpyAsync(x->rec.sc->sums, x->hio + 24, 5 * sizeof(double), cudaMemcpyHostToDevice, x->b.st));
+    CK(cudaMemcpyAsync(&x->rec.sc->ext_sums, x->hio + 29, sizeof(unsigned), cudaMemcpyHostToDevice, x->b.st));
+    return sync_and_check(x);
 }
 
 int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {

@@ -1301,12 +1301,15 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
 // ============================================================ forcing
 // get_rho_turb sums (turb_driver_mod.f90:158-186) over the step-start state,
 // per-block partial sums in FP64, reduced in a fixed order by k_force_reduce.
+// sums_only: the sums of this box for the host (slab ranks add them up,
+// turb_driver_mod.f90:184-189), whatever the drive flag; otherwise the sums
+// of a drive step, unless the host has set all ranks' sums (ext_sums).
 template <class T, bool ONE>
-__global__ void __launch_bounds__(kRedThreads) k_force_sums(BatchArgs ba) {
+__global__ void __launch_bounds__(kRedThreads) k_force_sums(BatchArgs ba, int sums_only) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindRed, local);
     const Scalars* sc = rp.sc;
-    if (!rp.active || !sc->drive) return;
+    if (!rp.active || (!sums_only && (!sc->drive || sc->ext_sums))) return;
     const T* __restrict__ S0 = (const T*)rp.S[0];
     const T* __restrict__ delv = (const T*)rp.delv;
     double* __restrict__ partials = rp.partials;
@@ -1339,12 +1342,42 @@ __global__ void __launch_bounds__(kRedThreads) k_force_sums(BatchArgs ba) {
     }
 }
 
+// The constant-energy normalisation of add_random_force from the five sums
+// (turb_driver_mod.f90:411-434): <rho delv> and constE, the larger root of
+// the kinetic-energy quadratic.
+__device__ __forceinline__ void force_normalise(Scalars* sc, const double* s, double dx, double edot, double dt_turb) {
+    double dx3 = dx * dx * dx;
+    if (s[0] <= 1.0e-20) {
+        sc->status |= 8u;
+        sc->constE = 0.0;
+        sc->mavg[0] = sc->mavg[1] = sc->mavg[2] = 0.0;
+        return;
+    }
+    sc->mavg[0] = s[2] * dx3;
+    sc->mavg[1] = s[3] * dx3;
+    sc->mavg[2] = s[4] * dx3;
+    double tmp1 = edot * dt_turb / dx3;
+    double tmp2 = sqrt(s[1] * s[1] + (4.0 * tmp1 * s[0]));
+    sc->constE = 0.5 * (-s[1] + tmp2) / s[0];
+}
+
 // Sum the per-block partials in block order, then the normalisation of
-// add_random_force (turb_driver_mod.f90:411-434) for one rank.
-static __global__ void k_force_reduce(BatchArgs ba) {
+// add_random_force (turb_driver_mod.f90:411-434).  The sums are this box's,
+// or all ranks' when the host set them (ext_sums, consumed here);
+// sums_only stops after storing this box's sums.
+static __global__ void k_force_reduce(BatchArgs ba, int sums_only) {
     const BoxRec rp = box_at(ba, blockIdx.x);   // one block of 32 threads per box
     Scalars* sc = rp.sc;
-    if (!rp.active || !sc->drive) return;
+    if (!rp.active || (!sums_only && !sc->drive)) return;
+    if (!sums_only && sc->ext_sums) {
+        if (threadIdx.x == 0) {
+            sc->ext_sums = 0u;
+            double s[5];
+            for (int q = 0; q < 5; ++q) s[q] = sc->sums[q];
+            force_normalise(sc, s, rp.dx, rp.edot, rp.dt_turb);
+        }
+        return;
+    }
     const double* __restrict__ partials = rp.partials;
     const int nblocks = rp.nred;
     const double dx = rp.dx, edot = rp.edot, dt_turb = rp.dt_turb;
@@ -1365,19 +1398,7 @@ static __global__ void k_force_reduce(BatchArgs ba) {
         }
         s[0] = 0.5 * s[0];
         for (int q = 0; q < 5; ++q) sc->sums[q] = s[q];
-        double dx3 = dx * dx * dx;
-        if (s[0] <= 1.0e-20) {
-            sc->status |= 8u;
-            sc->constE = 0.0;
-            sc->mavg[0] = sc->mavg[1] = sc->mavg[2] = 0.0;
-            return;
-        }
-        sc->mavg[0] = s[2] * dx3;
-        sc->mavg[1] = s[3] * dx3;
-        sc->mavg[2] = s[4] * dx3;
-        double tmp1 = edot * dt_turb / dx3;
-        double tmp2 = sqrt(s[1] * s[1] + (4.0 * tmp1 * s[0]));
-        sc->constE = 0.5 * (-s[1] + tmp2) / s[0];
+        if (!sums_only) force_normalise(sc, s, dx, edot, dt_turb);
     }
 }
 

@@ -180,8 +180,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     }
     if (b.drive_mode) {
         mark(b, kStForceSums);
-        k_force_sums<T, ONE><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a);
-        k_force_reduce<<<b.a.nbox, 32, 0, b.st>>>(b.a);
+        k_force_sums<T, ONE><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a, 0);
+        k_force_reduce<<<b.a.nbox, 32, 0, b.st>>>(b.a, 0);
         b.launches += 2;
     }
     // predictor: first-order fluxes, EMFs, half-dt update into the other buffer
@@ -244,6 +244,15 @@ template <class T, bool ONE>
 static cudaError_t run_max_speed_t(BatchDev& b) {
     k_cfl<T, ONE><<<grid_of<ONE>(b, kKindCell), kBX, 0, b.st>>>(b.a);
     b.launches += 1;
+    return cudaGetLastError();
+}
+
+// This box's forcing sums of the current state (no normalisation, any step).
+template <class T>
+cudaError_t run_force_sums(BatchDev& b) {
+    k_force_sums<T, true><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a, 1);
+    k_force_reduce<<<1, 32, 0, b.st>>>(b.a, 1);
+    b.launches += 2;
     return cudaGetLastError();
 }
 
@@ -329,6 +338,7 @@ cudaError_t run_init_uniform(cudaStream_t st, const BoxRec& r, int cur, double r
     template cudaError_t run_step<T>(BatchDev&, int);                              \
     template cudaError_t prepare_launch<T>(BatchDev&);                             \
     template cudaError_t run_max_speed<T>(BatchDev&);                              \
+    template cudaError_t run_force_sums<T>(BatchDev&);                             \
     template cudaError_t run_diag<T>(BatchDev&);                                   \
     template cudaError_t run_from_f64<T>(cudaStream_t, const double*, void*, int); \
     template cudaError_t run_to_f64<T>(cudaStream_t, const void*, double*, int);   \

@@ -59,7 +59,7 @@ struct Scalars {
     double smax_last, dvmax_last;
     double diag[6];
     unsigned int status;
-    unsigned int pad;
+    unsigned int ext_sums;           // sums[] hold all ranks' sums, set by the host for the next drive step
     unsigned long long floor_hits;
     // per-block maxima land in slot (block id mod kSlots); k_finalize folds them
     unsigned long long smax_slots[kSlots];

@@ -12,6 +12,23 @@ enter the speed maxima (imhd_set_geometry), so the new dt, min-reduced over
 ranks, equals the single-box dt, and the whole run equals the single-box run
 bit for bit in FP64.
 
+Forcing: on a drive step every slab adds up its forcing sums over its own
+planes (imhd_force_sums) and all ranks' totals set the kick's normalisation
+(imhd_set_force_sums), as the reference's all-reduce of get_rho_turb's sums
+does (turb_driver_mod.f90:184-189, 402-415).  The totals are added in a
+different order than one box adds its cells, so driven slab runs equal the
+single box to FP64 rounding rather than bit for bit.  The dt after a drive
+step is the minimum of the ranks' dts, each from its own max(c, smax +
+delv_max), as the reference's ranks take it (driver.f90:432-448 and the
+MIN all-reduce of share_dt); it can exceed one box's dt when smax and
+delv_max peak on different ranks.  With passive scalars
+a drive step differs at the global z boundary: a slab's halo planes are
+kicked with the rest, so the passive corrector of the planes next to the
+global boundary reads kicked velocities across it, where one box reads the
+unforced periodic image (the reference's ranks, for their part, read
+unforced ghost velocities at every rank boundary, turb_driver_mod.f90:
+437-453, passive_mod.f90:227-239).
+
 Dependency radius of one step along z: the half-step state needs the start
 state within 2 planes, the corrector's fluxes and corner EMFs need the
 half-step state within 3 (PLM) or 4 (PPM) planes, and the passive corrector
@@ -103,6 +120,12 @@ class LocalSlabs:
         p = self.dec.gather([p[2] for p in parts]) if self.npass else None
         return q, b, p
 
+    def set_force(self, delv):
+        """Force field of the global box (3, nz, ny, nx): every slab gets its
+        planes and halos."""
+        for r, box in enumerate(self.boxes):
+            box.set_force(np.ascontiguousarray(self.dec.scatter(delv, r)))
+
     def exchange(self):
         import torch
         bufs = []
@@ -117,9 +140,16 @@ class LocalSlabs:
         del bufs
         torch.cuda.synchronize()
 
-    def step(self, dt):
-        """One step of every slab, the halo exchange; the global next dt."""
-        dts = [box.step(dt) for box in self.boxes]
+    def step(self, dt, drive=False):
+        """One step of every slab, the halo exchange; the global next dt.  A
+        drive step first adds up the slabs' forcing sums (in rank order)."""
+        if drive:
+            total = np.zeros(5)
+            for box in self.boxes:
+                total = total + box.force_sums()
+            for box in self.boxes:
+                box.set_force_sums(total)
+        dts = [box.step(dt, drive) for box in self.boxes]
         self.exchange()
         return min(dts)
 
@@ -165,9 +195,14 @@ class RankSlab:
         self.box.unpack_planes(rlo, npl, recv_lo)
         self.box.unpack_planes(rhi, npl, recv_hi)
 
-    def step(self, dt):
+    def step(self, dt, drive=False):
         import torch
-        dt_local = self.box.step(dt)
+        if drive:
+            # all ranks' forcing sums (a SUM all-reduce) set the kick of this drive step
+            s = torch.tensor(np.asarray(self.box.force_sums(), dtype=np.float64), device=self.device)
+            self.dist.all_reduce(s, op=self.dist.ReduceOp.SUM)
+            self.box.set_force_sums(s.cpu().numpy())
+        dt_local = self.box.step(dt, drive)
         self.exchange()
         t = torch.tensor([dt_local], dtype=torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MIN)

@@ -32,9 +32,11 @@ def test_halo_width_and_too_thin_slabs():
 class HostSlab:
     """Stand-in for a device slab: planes of a (nf, nz, ny, nx) float64 array."""
 
-    def __init__(self, a, dt_local):
+    def __init__(self, a, dt_local, sums=None):
         self.a = a
         self.dt_local = dt_local
+        self.sums = sums
+        self.global_sums = None
 
     def pack_planes(self, z0, n):
         return torch.from_numpy(np.ascontiguousarray(self.a[:, z0:z0 + n]).reshape(-1).copy())
@@ -42,7 +44,13 @@ class HostSlab:
     def unpack_planes(self, z0, n, t):
         self.a[:, z0:z0 + n] = t.numpy().reshape(self.a.shape[0], n, *self.a.shape[2:])
 
-    def step(self, dt):
+    def force_sums(self):
+        return self.sums
+
+    def set_force_sums(self, s):
+        self.global_sums = np.asarray(s)
+
+    def step(self, dt, drive=False):
         return self.dt_local
 
 
@@ -61,6 +69,33 @@ def _rank_main(rank, world, port, q):
     ok = np.array_equal(local, dec.scatter(g, rank)) and dt == 0.1
     q.put((rank, ok))
     dist.destroy_process_group()
+
+
+def _drive_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dec = Decomposition((3, 2, 14), world, 3)
+    local = np.zeros((2, dec.local_nz(rank), 2, 3))
+    box = HostSlab(local, 0.1, sums=np.arange(1.0, 6.0) * (rank + 1))
+    RankSlab(dec, rank, box, dist).step(1.0, drive=True)
+    expect = np.arange(1.0, 6.0) * sum(r + 1 for r in range(world))
+    q.put((rank, box.global_sums is not None and np.array_equal(box.global_sums, expect)))
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_add_up_forcing_sums_on_drive_steps(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29600 + world + (os.getpid() % 1000)
+    procs = [ctx.Process(target=_drive_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert all(res[r] for r in range(world)), res
 
 
 @pytest.mark.parametrize("world", [2, 3])
