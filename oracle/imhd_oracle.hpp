@@ -77,7 +77,7 @@ struct Config {
     int nb = 6;                 // ghost layers (constants_mod.f90:12)
     double sound_speed = 1.0;   // constants_mod.f90:35
     int riemann = 1;            // 1 Roe, 2 HLLD, 3 HLLE (constants_mod.f90:57)
-    int ppm = 0;                // 0 PLM (north-star path), 1 PPM (reference default)
+    int ppm = 0;                // 0 PLM (the benchmarked path), 1 PPM (reference default)
     int npass = 0;              // passive scalars (constants_mod.f90:63)
     double edot = 1.0e-3;       // constants_mod.f90:44
     double dt_turb = 0.05;      // constants_mod.f90:42

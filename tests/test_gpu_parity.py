@@ -190,7 +190,7 @@ def test_fp32_within_1e5_of_fp64_oracle(riemann):
     for name in ("q", "b", "p"):
         ref = o[name]
         err = rel_l1(g[name], ref)
-        # fields that are identically zero in the reference are judged in absolute terms
+        # fields that are identically zero in the reference are compared in absolute terms
         assert np.all(err <= 1e-5), (name, err)
 
 
