@@ -762,10 +762,14 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
 }
 
 // A table's box goes to the bulk-copy fed update when its rows are whole
-// 128-cell tiles and the bases its copies read from are 16-byte aligned (both
+// 128-cell tiles (or 64-cell tiles with an even row count: a block then takes
+// two rows) and the bases its copies read from are 16-byte aligned (both
 // update kernels decide from the same record, so exactly one takes the box).
+__host__ __device__ __forceinline__ int tma_row_tile(int nx, int ny) {
+    return nx % kTmaTile == 0 ? kTmaTile : (nx % (kTmaTile / 2) == 0 && ny % 2 == 0) ? kTmaTile / 2 : 0;
+}
 __device__ __forceinline__ bool update_by_tma(const BoxRec& r) {
-    return r.nx % kTmaTile == 0 && (((uintptr_t)r.S[0] | (uintptr_t)r.F | (uintptr_t)r.E) & 15) == 0;
+    return tma_row_tile(r.nx, r.ny) > 0 && (((uintptr_t)r.S[0] | (uintptr_t)r.F | (uintptr_t)r.E) & 15) == 0;
 }
 
 // A thread walks a column of kSegZ cells along z; the z-face fluxes, the
@@ -896,12 +900,15 @@ constexpr unsigned kStatusWait = 16u;        // IMHD_S_WAIT
 constexpr long long kTmaSpin = 1ll << 24;   // try_wait polls before a wait gives up
 template <class T>
 constexpr int tma_row_stride() { return kTmaTile + 16 / (int)sizeof(T); }   // a 16-byte halo slot + the row
-template <class T>
-constexpr int tma_copy_bytes() { return kTmaRows * kTmaTile * (int)sizeof(T) + kTmaHalos * 16; }
-template <class T>
-constexpr int tma_stage_bytes() { return (kTmaRows * tma_row_stride<T>() * (int)sizeof(T) + 127) / 128 * 128; }
-template <class T>
-constexpr size_t update_tma_smem_bytes() { return 2 * (size_t)tma_stage_bytes<T>(); }
+// a block stages kTmaTile / TW rows of TW-cell segments
+template <class T, int TW>
+constexpr int tma_copy_bytes() { return kTmaRows * kTmaTile * (int)sizeof(T) + (kTmaTile / TW) * kTmaHalos * 16; }
+template <class T, int TW>
+constexpr int tma_stage_bytes() {
+    return ((kTmaTile / TW) * kTmaRows * (TW + 2 * (16 / (int)sizeof(T))) * (int)sizeof(T) + 127) / 128 * 128;
+}
+template <class T, int TW>
+constexpr size_t update_tma_smem_bytes() { return 2 * (size_t)tma_stage_bytes<T, TW>(); }
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
@@ -933,13 +940,14 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
                  : "memory");
 }
 
-template <class T, bool ZR, bool ONE>
+template <class T, bool ZR, bool ONE, int TW>
 __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     k_update_tma(BatchArgs ba, double dt_scale, int final_stage) {
     extern __shared__ __align__(128) unsigned char tma_smem[];
     __shared__ __align__(8) unsigned long long bars[2];
+    constexpr int RB = kTmaTile / TW;    // rows per block
     int local;
-    const BoxRec rp = resolve<ONE>(ba, kKindUpdTma, local);
+    const BoxRec rp = resolve<ONE>(ba, TW == kTmaTile ? kKindUpdTma : kKindUpdTma64, local);
     Scalars* sc = rp.sc;
     if (!rp.active || (!ONE && !update_by_tma(rp))) return;
     const Dims dm = dims_of(rp);
@@ -950,18 +958,19 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     const T asqr = (T)(rp.cs * rp.cs);
     const int do_cfl = final_stage && !sc->drive;
     const int t = (int)threadIdx.x;
-    int i0, j, seg;
-    if constexpr (ONE) {   // grid (nx / 128, ny, z segments)
-        i0 = (int)blockIdx.x * kTmaTile;
-        j = (int)blockIdx.y;
+    const int lx = t % TW, ly = t / TW;
+    int i0, j0, seg;
+    if constexpr (ONE) {   // grid (nx / TW, ny / RB, z segments)
+        i0 = (int)blockIdx.x * TW;
+        j0 = (int)blockIdx.y * RB;
         seg = (int)blockIdx.z;
     } else {
-        const int nbx = dm.nx / kTmaTile, rest = local / nbx;
-        i0 = (local % nbx) * kTmaTile;
-        j = rest % dm.ny;
-        seg = rest / dm.ny;
+        const int nbx = dm.nx / TW, nby = dm.ny / RB, rest = local / nbx;
+        i0 = (local % nbx) * TW;
+        j0 = (rest % nby) * RB;
+        seg = rest / nby;
     }
-    const int i = i0 + t;
+    const int i = i0 + lx, j = j0 + ly;
     const int k0 = seg * kSegZ, k1 = min(k0 + kSegZ, dm.nz);
     const int n = dm.n, plane = dm.nx * dm.ny;
     const int jm = wrap_dn(j, dm.ny);
@@ -974,17 +983,18 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
         mbar_init_fence();
     }
     __syncthreads();
-    // operand rows of plane k into stage g: row r (and its halo) by lane r of warp 0
-    constexpr int RS = tma_row_stride<T>();
+    // operand rows of plane k into stage g: row R = (block row) * 29 + r, and
+    // its halo, by lane R % 32 of warp 0
+    constexpr int RS = TW + 2 * HE;
     auto issue = [&](int g, int k) {
-        T* rows = (T*)(tma_smem + (size_t)g * tma_stage_bytes<T>());
+        T* rows = (T*)(tma_smem + (size_t)g * tma_stage_bytes<T, TW>());
         unsigned long long* bar = &bars[g];
-        if (t == 0) mbar_expect_tx(bar, (unsigned)tma_copy_bytes<T>());
+        if (t == 0) mbar_expect_tx(bar, (unsigned)tma_copy_bytes<T, TW>());
         __syncwarp();
-        if (t < kTmaRows) {
-            const int r = t;
+        for (int R = t; R < RB * kTmaRows; R += 32) {
+            const int r = R % kTmaRows, jrow = j0 + R / kTmaRows, jm = wrap_dn(jrow, dm.ny);
             const T* base;
-            int jr = j;
+            int jr = jrow;
             if (r < 4) base = fld(S0, r, n);
             else if (r < 7) base = fld(S0, 3 + r, n);                                        // fields 7-9
             else if (r < 11) base = F + (size_t)(r - 7) * n;                                  // x fluxes
@@ -996,10 +1006,10 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
             else if (r == 27) { base = E; jr = jm; }
             else { base = E + 2 * (size_t)n; jr = jm; }
             const size_t ofs = (size_t)dm.nx * (jr + (size_t)dm.ny * k);
-            bulk_g2s(rows + r * RS + HE, base + i0 + ofs, kTmaTile * (unsigned)sizeof(T), bar);
+            bulk_g2s(rows + R * RS + HE, base + i0 + ofs, TW * (unsigned)sizeof(T), bar);
             // rows whose left neighbour is read: x fluxes, bx, Ey, Ez and Ez of row j-1
             if ((r >= 7 && r <= 10) || r == 4 || r == 20 || r == 21 || r == 28)
-                bulk_g2s(rows + r * RS, base + ih + ofs, 16u, bar);
+                bulk_g2s(rows + R * RS, base + ih + ofs, 16u, bar);
         }
     };
     if (t < 32) issue(0, k0);
@@ -1033,7 +1043,7 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
             atomicOr(&sc->status, kStatusWait);
         }
         if (ok) {
-            const T* rows = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T>()) + HE + t;
+            const T* rows = (const T*)(tma_smem + (size_t)g * tma_stage_bytes<T, TW>()) + ly * kTmaRows * RS + HE + lx;
             auto at = [&](int r) { return rows[r * RS]; };
             auto xm = [&](int r, int) { return rows[r * RS - 1]; };
             const int c = r0 + k * plane;

@@ -83,19 +83,32 @@ static void ensure_xrow_attr() {
 }
 
 // The TMA-fed update's two stages exceed 48 KiB of shared memory in FP64.
+template <class T, int TW>
+static void set_update_tma_attr() {
+    const int bytes = (int)update_tma_smem_bytes<T, TW>();
+    cudaFuncSetAttribute(k_update_tma<T, false, true, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_update_tma<T, true, true, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_update_tma<T, false, false, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_update_tma<T, true, false, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 template <class T>
 static void ensure_update_tma_attr() {
     static bool attr_set[64] = {};   // per precision and device
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        const int bytes = (int)update_tma_smem_bytes<T>();
-        cudaFuncSetAttribute(k_update_tma<T, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(k_update_tma<T, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(k_update_tma<T, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(k_update_tma<T, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        set_update_tma_attr<T, kTmaTile>();
+        set_update_tma_attr<T, kTmaTile / 2>();
         if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
+}
+
+template <class T, bool ONE, int TW>
+static void launch_update_tma(BatchDev& b, dim3 g, double dt_scale, int final_stage) {
+    const size_t smem = update_tma_smem_bytes<T, TW>();
+    if (b.any_zrange) k_update_tma<T, true, ONE, TW><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+    else k_update_tma<T, false, ONE, TW><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
+    b.launches += 1;
 }
 
 // Update of one stage: the TMA-fed kernel for a single box whose rows are
@@ -108,24 +121,24 @@ static void launch_update(BatchDev& b, double dt_scale, int final_stage) {
     // the bulk copies need 16-byte aligned sources: every row of a 128-cell
     // tile starts on one when the field bases do
     const bool aligned = ((uintptr_t)b.a.one.S[0] | (uintptr_t)b.a.one.F | (uintptr_t)b.a.one.E) % 16 == 0;
-    const size_t smem = update_tma_smem_bytes<T>();
-    if (ONE && aligned && b.a.one.nx % kTmaTile == 0) {
+    const int tw = tma_row_tile(b.a.one.nx, b.a.one.ny);
+    if (ONE && aligned && tw > 0) {
         ensure_update_tma_attr<T>();
-        const dim3 g((unsigned)(b.a.one.nx / kTmaTile), (unsigned)b.a.one.ny, (unsigned)((b.a.one.nz + kSegZ - 1) / kSegZ));
-        if (b.any_zrange) k_update_tma<T, true, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-        else k_update_tma<T, false, true><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-        b.launches += 1;
+        const dim3 g((unsigned)(b.a.one.nx / tw), (unsigned)(b.a.one.ny / (kTmaTile / tw)),
+                     (unsigned)((b.a.one.nz + kSegZ - 1) / kSegZ));
+        if (tw == kTmaTile) launch_update_tma<T, ONE, kTmaTile>(b, g, dt_scale, final_stage);
+        else launch_update_tma<T, ONE, kTmaTile / 2>(b, g, dt_scale, final_stage);
         return;
     }
     if (b.any_zrange) k_update<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
     else k_update<T, ONE, false><<<gz, kBX, 0, b.st>>>(b.a, dt_scale, final_stage);
     b.launches += 1;
-    if (!ONE && b.totals[kKindUpdTma] > 0) {
+    if (!ONE && (b.totals[kKindUpdTma] > 0 || b.totals[kKindUpdTma64] > 0)) {
         ensure_update_tma_attr<T>();
-        const unsigned g = (unsigned)b.totals[kKindUpdTma];
-        if (b.any_zrange) k_update_tma<T, true, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-        else k_update_tma<T, false, false><<<g, kTmaTile, smem, b.st>>>(b.a, dt_scale, final_stage);
-        b.launches += 1;
+        if (b.totals[kKindUpdTma] > 0)
+            launch_update_tma<T, ONE, kTmaTile>(b, dim3((unsigned)b.totals[kKindUpdTma]), dt_scale, final_stage);
+        if (b.totals[kKindUpdTma64] > 0)
+            launch_update_tma<T, ONE, kTmaTile / 2>(b, dim3((unsigned)b.totals[kKindUpdTma64]), dt_scale, final_stage);
     }
 }
 

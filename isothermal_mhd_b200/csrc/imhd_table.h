@@ -29,6 +29,10 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
     if (kind == kKindCellZ) return nbx * nby * ceil_div(r.nz, 1 << r.segzs);
     if (kind == kKindRed) return r.nred;
     if (kind == kKindUpdTma) return r.nx % kTmaTile == 0 ? (long)(r.nx / kTmaTile) * r.ny * ceil_div(r.nz, kSegZ) : 0;
+    if (kind == kKindUpdTma64)
+        return (r.nx % kTmaTile != 0 && r.nx % (kTmaTile / 2) == 0 && r.ny % 2 == 0)
+                   ? (long)(r.nx / (kTmaTile / 2)) * (r.ny / 2) * ceil_div(r.nz, kSegZ)
+                   : 0;
     int scheme = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
     if (scheme_of(r.riemann, r.recon) != scheme) return 0;

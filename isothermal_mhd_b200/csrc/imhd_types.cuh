@@ -34,7 +34,8 @@ enum Kind {
     kKindSolver0 = 2,  // + 5*(scheme-1) + {z column (predictor), x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
     kKindCellZ = 32,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
     kKindUpdTma = 33,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
-    kKinds = 34
+    kKindUpdTma64 = 34,// pairs of 64-cell row segments per z segment of it (rows of 64(2k+1) cells, even ny)
+    kKinds = 35
 };
 // A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
 // (0 PLM, 1 PPM): scheme = solver + 3 * recon, 1..kSchemes.

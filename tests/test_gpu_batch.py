@@ -132,7 +132,7 @@ def test_online_tuning_changes_no_bits(precision):
     # the tuner times eight decomposition settings on the first eight steps;
     # the result equals the untuned run bit for bit
     cases = [((32, 24, 40), "roe", 2, "plm"), ((48, 32, 32), "hlld", 0, "ppm"), ((20, 20, 20), "hlle", 1, "plm"),
-             ((128, 12, 16), "roe", 1, "plm")]
+             ((128, 12, 16), "roe", 1, "plm"), ((64, 10, 16), "hlld", 1, "plm")]
     out = []
     for tune in (True, False):
         cfgs = [make_config(n, precision=precision, riemann=s, npass=np_, cour=0.4, recon=r) for n, s, np_, r in cases]

@@ -71,13 +71,15 @@ def test_fp64_bit_exact_32_roe():
     assert_exact(g, o)
 
 
-# Rows that are whole 128-cell tiles take the TMA-fed update and passive
-# predictor kernels (bulk copies of each plane's rows into shared memory);
+# Rows that are whole 128-cell tiles (or 64-cell tiles with an even row
+# count, two rows per block) take the TMA-fed update kernel (bulk copies of
+# each plane's rows into shared memory);
 # nz = 18 and 20 leave a partial last z segment, the rows next to j = 0 and
 # j = ny - 1 wrap, and the first and last tiles of each row read their x
 # neighbours from the periodic images.
 @pytest.mark.parametrize("riemann,n,npass", [("roe", (128, 12, 20), 1), ("hlld", (256, 12, 18), 2),
-                                             ("hlle", (256, 12, 18), 4), ("roe", (128, 12, 18), 0)])
+                                             ("hlle", (256, 12, 18), 4), ("roe", (128, 12, 18), 0),
+                                             ("hlld", (64, 12, 18), 1), ("roe", (192, 14, 17), 2)])
 def test_fp64_bit_exact_tma_update_rows(riemann, n, npass):
     ic = problems.smooth_wave_box(n, npass=max(npass, 1))
     if npass == 0:
