@@ -881,16 +881,19 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
 }
 
 // ------------------------------------------------------------ update, TMA-fed
-// The same update for single boxes whose rows are whole 128-cell tiles: a
-// block owns a 128-cell row segment and walks kSegZ planes; thread 0 streams
-// each plane's operands into shared memory with bulk asynchronous copies
-// (cp.async.bulk, completion counted on an mbarrier), one plane ahead of the
-// plane being computed, so that the loads' latency overlaps the arithmetic
-// without registers held for them.  Per plane: 29 row segments of 128 cells
-// (22 fields of row j, 7 of row j-1) and 8 16-byte segments that end at the
-// cell left of the tile (the periodic image at i = nx-1 for the first tile),
-// each stored just in front of its row so that the left neighbour of every
-// cell is the element before it.  Lane r of warp 0 issues row r.
+// The same update for boxes whose rows are whole 128-cell tiles (TW = 128),
+// or 64-cell tiles with an even row count (TW = 64, two rows per block): a
+// block owns 128 cells of one or two rows and walks kSegZ planes; warp 0
+// streams each plane's operands into shared memory with bulk asynchronous
+// copies (cp.async.bulk, completion counted on an mbarrier), one plane ahead
+// of the plane being computed, so that the loads' latency overlaps the
+// arithmetic without registers held for them.  Per plane and row: 29 row
+// segments (22 fields of row j, 7 of row j-1) and 8 16-byte segments that end
+// at the cell left of the tile (the periodic image at i = nx-1 for the first
+// tile), each stored just in front of its row so that the left neighbour of
+// every cell is the element before it.  Lane R % 32 of warp 0 issues row R.
+// Single boxes launch it alone; a table launches it beside k_update, which
+// skips the boxes it takes (update_by_tma).
 // Every wait is bounded: on time-out the kernel sets IMHD_S_WAIT in the
 // status word, skips the arithmetic and drains its copies with a bounded
 // wait before it exits.
