@@ -5,7 +5,8 @@
  * whose hot path is a handful of module procedures acting on module-global
  * arrays.  This header is the drop-in boundary for that path: a Fortran
  * driver binds these entry points through ISO_C_BINDING (the binding module
- * is in INTEGRATION.md), a C/C++ or Python (ctypes) host binds them directly.
+ * declares these prototypes as BIND(C) interfaces), a C/C++ or Python
+ * (ctypes) host binds them directly.
  *
  * Conventions
  *  - Every call returns an int status: IMHD_OK (0) or a positive IMHD_E_* code;
@@ -37,7 +38,7 @@ extern "C" {
 #define IMHD_E_ARG 1        /* bad argument or configuration */
 #define IMHD_E_CUDA 2       /* CUDA runtime error (no device, launch failure) */
 #define IMHD_E_NOMEM 3      /* device allocation failed */
-#define IMHD_E_PHYSICS 4    /* zero max speed or bad forcing normalisation */
+#define IMHD_E_PHYSICS 4    /* non-finite state, zero max speed or bad forcing normalisation */
 #define IMHD_E_STATE 5      /* call out of order (e.g. drive without a force field) */
 
 /* Riemann solvers (riemann_solver_type, constants_mod.f90:57) */
@@ -51,7 +52,7 @@ extern "C" {
 
 /* status-word bits reported by imhd_status */
 #define IMHD_S_FLOOR 1u     /* a density fell below 1e-20 and was floored (vanleer_mod.f90:3243-3262) */
-#define IMHD_S_NAN 2u       /* a non-finite max speed was seen */
+#define IMHD_S_NAN 2u       /* a non-finite updated state or max speed was seen */
 #define IMHD_S_ZERO_SPEED 4u/* max speed < 1e-20 (vanleer_mod.f90:3328) */
 #define IMHD_S_FORCE 8u     /* forcing quadratic term <= 1e-20 (turb_driver_mod.f90:420) */
 #define IMHD_S_WAIT 16u     /* a bounded wait for an asynchronous copy in a kernel gave up; the step is not valid */
@@ -117,7 +118,10 @@ int imhd_set_force_sums(imhd_box* box, const double* sums);
  * passive_solve_3d (passive_mod.f90:118-201), the periodic ghost fill and
  * compute_new_time_step (driver.f90:55-131, 432-448).  On return *dt_next holds
  * the new local dt = COUR*dx/cmax with COUR halved after a drive step
- * (driver.f90:109); the caller applies MIN(t_end - t, dt) (driver.f90:475). */
+ * (driver.f90:109); the caller applies MIN(t_end - t, dt) (driver.f90:475).
+ * A step that leaves a non-finite state or max speed returns IMHD_E_PHYSICS
+ * (IMHD_S_NAN stays set in imhd_status); the reference has no such check and
+ * would carry the NaN into its next dt. */
 int imhd_step(imhd_box* box, double dt, int drive_next, double* dt_next);
 
 /* cmax of the current state alone: get_max_speed_vanleer with smax = 0
@@ -365,23 +369,29 @@ int imhd_server_stats(imhd_server* server, double* out, int n);
 int imhd_server_stop(imhd_server* server, int drain);
 void imhd_server_destroy(imhd_server* server);
 
-/* One undriven time step, like imhd_step, for callers that cannot allocate
- * device memory: hosts that own every device buffer (pool allocators,
- * OpenACC / CUDA Fortran managed arrays), code running inside a CUDA graph
- * capture, allocation-free real-time loops.  No reference counterpart: the
- * reference allocates its work arrays itself (vanleer_mod.f90:169-244).
+/* One undriven time step with PLM reconstruction, like imhd_step, for callers
+ * that cannot allocate device memory: hosts that own every device buffer
+ * (pool allocators, OpenACC or CUDA Fortran arrays whose runtime keeps the
+ * device heap to itself) and real-time loops that forbid allocation after
+ * start-up.  No reference counterpart: the reference allocates its work
+ * arrays itself (vanleer_mod.f90:169-244).
  * The caller passes device buffers: state_in (read) and state_out (written),
  * distinct, each 10 + npass fields of nx*ny*nz elements of the precision's
  * type in the library's layout (rho, mx, my, mz, Bx_cc, By_cc, Bz_cc,
  * Bx_face, By_face, Bz_face, passive scalars; x fastest).  dt is read from
- * the host, *dt_next (host) receives COUR*dx/cmax, stream may be NULL.
+ * the host, *dt_next (host) receives COUR*dx/cmax, stream may be NULL; the
+ * call returns when the step is done.  Reconstruction is always PLM and
+ * there is no forcing kick (use imhd_create / imhd_step for PPM or driving).
  * The step's work arrays live in one 48 MiB file-scope device array held by
  * every GPU that loads the library until exit; boxes needing more
- * ((21 + npass) * nx*ny*nz * element size + 56 KiB: 64^3 in FP64, about 80^3
- * in FP32 with two passives) are rejected with IMHD_E_ARG.  All calls on a
- * device share that array: calls that overlap on the GPU race.  The first
- * call on a device looks up the array's device address; make it before any
- * stream capture starts. */
+ * ((21 + npass) * nx*ny*nz * element size + 56 KiB: 64^3 in FP64 with at most
+ * two passive scalars, about 80^3 in FP32 with two) are rejected with
+ * IMHD_E_ARG.  All calls on a device share that array and leave their
+ * contents in it: calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's device address and keeps it for the life of
+ * the process, so the library must not be used across a cudaDeviceReset.
+ * A non-finite result returns IMHD_E_PHYSICS; floored densities are not
+ * reported by this entry point. */
 int imhd_step_static(int precision, int nx, int ny, int nz, int riemann, int npass, double sound_speed,
                      double cour, const void* state_in, void* state_out, double dt, double* dt_next,
                      void* stream);

@@ -448,6 +448,7 @@ int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
     if (dt_next) *dt_next = x->hio[1];
     unsigned st = *(unsigned*)(x->hio + 2);
     if (st & IMHD_S_WAIT) return fail(IMHD_E_CUDA, "a bounded wait for an asynchronous copy gave up");
+    if (st & IMHD_S_NAN) return fail(IMHD_E_PHYSICS, "non-finite state or max speed: the step is not valid");
     if (st & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
     if (st & IMHD_S_FORCE) return fail(IMHD_E_PHYSICS, "bad value in turbulence driver energy normalisation");
     return IMHD_OK;

@@ -202,9 +202,9 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     for_schemes([&](auto s) { launch_fluxes_pred<T, s.value, ONE>(b); });
     mark(b, kStPredEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
-    mark(b, kStPredUpdate);
-    launch_update<T, ONE>(b, 0.5, 0);
     b.launches += 1;
+    mark(b, kStPredUpdate);
+    launch_update<T, ONE>(b, 0.5, 0);   // counts its own launches
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
     mark(b, kStCorrFluxX);
@@ -215,9 +215,9 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     for_schemes([&](auto s) { launch_fluxes_corr_march<T, s.value, 2, ONE>(b); });
     mark(b, kStCorrEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
+    b.launches += 1;
     mark(b, kStFinalUpdate);
     launch_update<T, ONE>(b, 1.0, 1);
-    b.launches += 1;
     if (b.drive_mode) {
         mark(b, kStForceKick);
         k_force_kick<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);

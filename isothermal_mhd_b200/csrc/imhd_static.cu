@@ -2,27 +2,29 @@
 //
 // Who needs it: hosts that own all device memory and may not call cudaMalloc
 // themselves or let a library do it -- a Fortran or C driver whose arrays
-// live in a pool or are managed by OpenACC / CUDA Fortran, code that runs
-// while a stream is being captured into a CUDA graph (cudaMalloc is not
-// permitted then), and real-time loops that forbid allocation after start-up.
-// They pass the state in and receive the state out; the step's work arrays
-// (interface fluxes, corner EMFs, half-step passive scalars and the reduction
-// scalars) live in one file-scope device array instead of in per-box
-// allocations.
+// live in a pool or are managed by OpenACC / CUDA Fortran, whose runtime keeps
+// the device heap to itself -- and real-time loops that forbid allocation
+// after start-up.  They pass the state in and receive the state out; the
+// step's work arrays (interface fluxes, corner EMFs, half-step passive
+// scalars and the reduction scalars) live in one file-scope device array
+// instead of in per-box allocations.  The step is undriven, with PLM
+// reconstruction.
 //
 // Limits and sharing:
 //  * the scratch array holds kStaticScratchBytes (48 MiB) on every GPU that
 //    loads the library, until the process exits; a box needs
 //    (21 + npass) * nx*ny*nz * (4 or 8) bytes plus 56 KiB, i.e. up to 64^3 in
-//    FP64 or about 80^3 in FP32 with two passive scalars.  Larger boxes are
-//    rejected with IMHD_E_ARG; use imhd_create / imhd_step for them;
+//    FP64 with at most two passive scalars or about 80^3 in FP32 with two.
+//    Larger boxes are rejected with IMHD_E_ARG; use imhd_create / imhd_step
+//    for them;
 //  * every call on a device uses the same array and leaves its contents
 //    behind; the reduction scalars are cleared at the start of each call.
 //    Calls that overlap on the GPU (two streams, two host threads) race on
 //    the array and must be serialised by the caller;
 //  * the first call on a device looks up the array's device address (with
-//    that device current) and caches it; make that first call before any
-//    stream capture begins.
+//    that device current) and keeps it for the life of the process: a
+//    cudaDeviceReset would leave it stale, so the library must not be used
+//    across one.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -93,7 +95,7 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     if (need > kStaticScratchBytes)
         return fail(IMHD_E_ARG, "box needs " + std::to_string(need) + " bytes of step scratch but imhd_step_static holds " +
                                     std::to_string(kStaticScratchBytes) +
-                                    " (at most 64^3 in FP64 or about 80^3 in FP32 with two passive scalars); "
+                                    " (at most 64^3 in FP64 with two passive scalars, about 80^3 in FP32 with two); "
                                     "use imhd_create / imhd_step");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -146,6 +148,7 @@ extern "C" int imhd_step_static(int precision, int nx, int ny, int nz, int riema
     if (e == cudaSuccess) e = cudaStreamSynchronize(b.st);
     if (e != cudaSuccess) return fail(IMHD_E_CUDA, std::string("imhd_step_static: ") + cudaGetErrorString(e));
     if (status & IMHD_S_WAIT) return fail(IMHD_E_CUDA, "a bounded wait for an asynchronous copy gave up");
+    if (status & IMHD_S_NAN) return fail(IMHD_E_PHYSICS, "non-finite state or max speed: the step is not valid");
     if (status & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
     if (dt_next) *dt_next = host_io[1];
     return IMHD_OK;

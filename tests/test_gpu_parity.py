@@ -262,3 +262,44 @@ def test_driven_run_with_device_reference_generator_matches_oracle():
     assert rec.drive_steps == drives and len(drives) >= 2
     for g, r in ((qg, qo), (bg, bo), (pg, po)):
         assert np.all(rel_l1(g, r) <= 1e-12), rel_l1(g, r)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_non_finite_state_returns_physics_error(precision):
+    # a NaN density poisons its neighbours' fluxes: the step that produces the
+    # non-finite state returns IMHD_E_PHYSICS at once (not on the next call)
+    from isothermal_mhd_b200 import Box, ImhdError
+    n = 16
+    q, b, p = problems.smooth_wave_box(n, npass=1)
+    q[0, 4, 6, 9] = np.nan
+    with Box(n, precision=precision, riemann="roe", npass=1, cour=0.4) as box:
+        box.upload(q, b, p)
+        with pytest.raises(ImhdError) as ei:
+            box.step(1e-4)
+        assert "IMHD_E_PHYSICS" in str(ei.value) and "non-finite" in str(ei.value)
+        assert box.status()["nan"]
+
+
+@pytest.mark.parametrize("ic_kind,riemann", [("smooth", "roe"), ("turbulent", "roe"), ("turbulent", "hlld")])
+def test_fp32_64cubed_100_steps_within_1e5_of_fp64(ic_kind, riemann):
+    # the north-star accuracy bound at a size the test run affords: 64^3, 100
+    # steps, relative L1 <= 1e-5 per field of the FP32 step against the FP64
+    # GPU path (itself bit-exact with the oracle at 64^3 x 100 steps, see
+    # test_gpu_golden), on the FP64 run's dt sequence.  "turbulent": rms Mach 2
+    # solenoidal velocity, B0 = (0.5, 0, 0), two passive scalars U[0, 1), and
+    # three forcing kicks.
+    from isothermal_mhd_b200 import forcing
+    n, steps = 64, 100
+    if ic_kind == "smooth":
+        ic, force, drive_at = problems.smooth_wave_box(n, npass=1), None, ()
+    else:
+        f = forcing.OUForcing(n, seed=11)
+        q, b, p = forcing.turbulent_box(n, mach=2.0, b0=(0.5, 0.0, 0.0), npass=2, seed=11, forcing=f)
+        f.advance(0.05)
+        ic, force, drive_at = (q, b, p), f.field(rms=1.0), (25, 50, 75)
+    g64 = gpu_run(ic, n, riemann, steps, precision=64, force=force, drive_at=drive_at, edot=4.0)
+    g32 = gpu_run(ic, n, riemann, steps, precision=32, force=force, drive_at=drive_at, edot=4.0, dts=g64["dts"])
+    assert not g64["status"]["nan"] and not g32["status"]["nan"]
+    for name in ("q", "b", "p"):
+        err = rel_l1(g32[name], g64[name])
+        assert np.all(err <= 1e-5), (name, err)
