@@ -46,9 +46,13 @@ extern "C" {
 #define IMHD_HLLD 2
 #define IMHD_HLLE 3
 
-/* interface reconstruction (piecewise_parabolic, vanleer_mod.f90:83) */
+/* interface reconstruction: piecewise_parabolic (vanleer_mod.f90:83) of the
+ * characteristic variables (the reference's default, :1488-1818) or, with
+ * primitive_reconstruction (:84), of the primitive variables (:1144-1485) */
 #define IMHD_PLM 0
 #define IMHD_PPM 1
+#define IMHD_PLM_PRIM 2
+#define IMHD_PPM_PRIM 3
 
 /* status-word bits reported by imhd_status */
 #define IMHD_S_FLOOR 1u     /* a density fell below 1e-20 and was floored (vanleer_mod.f90:3243-3262) */
@@ -61,7 +65,7 @@ typedef struct imhd_config {
     int nx, ny, nz;        /* interior cells per axis (constants_mod.f90:9-11) */
     int precision;         /* 64: FP64 everywhere; 32: FP32 bulk, FP64 reductions */
     int riemann;           /* IMHD_ROE / IMHD_HLLD / IMHD_HLLE */
-    int recon;             /* IMHD_PLM or IMHD_PPM */
+    int recon;             /* IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM */
     int npass;             /* passive scalars, 0..8 (constants_mod.f90:63) */
     double sound_speed;    /* isothermal sound speed (constants_mod.f90:35) */
     double cour;           /* COUR_def (constants_mod.f90:16) */

@@ -15,6 +15,10 @@ IMHD_OK = 0
 IMHD_E_PHYSICS = 4
 ERRORS = {1: "IMHD_E_ARG", 2: "IMHD_E_CUDA", 3: "IMHD_E_NOMEM", 4: "IMHD_E_PHYSICS", 5: "IMHD_E_STATE"}
 S_FLOOR, S_NAN, S_ZERO_SPEED, S_FORCE = 1, 2, 4, 8
+# interface reconstruction (imhd_config.recon): characteristic PLM / PPM (the
+# reference's default, vanleer_mod.f90:1488-1818) or primitive-variable PLM / PPM
+# (primitive_reconstruction, :1144-1485)
+RECON = {"plm": 0, "ppm": 1, "plm-prim": 2, "ppm-prim": 3}
 
 # Every symbol declared in include/imhd.h (checked by tests/test_capi_symbols.py).
 EXPORTS = (

@@ -12,7 +12,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import IMHD_E_PHYSICS, ImhdConfig, check, lib
+from ._lib import IMHD_E_PHYSICS, RECON, ImhdConfig, check, lib
 from .box import RIEMANN, _dptr
 
 
@@ -24,7 +24,7 @@ def make_config(n, precision=32, riemann="roe", npass=0, sound_speed=1.0, cour=0
     c.nx, c.ny, c.nz = int(nx), int(ny), int(nz)
     c.precision = int(precision)
     c.riemann = RIEMANN[riemann] if isinstance(riemann, str) else int(riemann)
-    c.recon = {"plm": 0, "ppm": 1}[recon] if isinstance(recon, str) else int(recon)
+    c.recon = RECON[recon] if isinstance(recon, str) else int(recon)
     c.npass = int(npass)
     c.sound_speed = float(sound_speed)
     c.cour = float(cour)

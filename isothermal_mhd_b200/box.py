@@ -50,7 +50,7 @@ class Box:
         cfg.nx, cfg.ny, cfg.nz = int(nx), int(ny), int(nz)
         cfg.precision = int(precision)
         cfg.riemann = RIEMANN[riemann] if isinstance(riemann, str) else int(riemann)
-        cfg.recon = {"plm": 0, "ppm": 1}[recon]
+        cfg.recon = _lib.RECON[recon]
         cfg.npass = int(npass)
         cfg.sound_speed = float(sound_speed)
         cfg.cour = float(cour)

@@ -176,7 +176,7 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         if ((double)c.nx * c.ny * c.nz >= 2147483647.0) return bfail(IMHD_E_ARG, "box too large");
         if (c.precision != 32 && c.precision != 64) return bfail(IMHD_E_ARG, "precision must be 32 or 64");
         if (c.riemann < 1 || c.riemann > 3) return bfail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
-        if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) return bfail(IMHD_E_ARG, "recon must be IMHD_PLM or IMHD_PPM");
+        if (c.recon < IMHD_PLM || c.recon > IMHD_PPM_PRIM) return bfail(IMHD_E_ARG, "recon must be IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM");
         if (c.npass < 0 || c.npass > imhd::kMaxPass) return bfail(IMHD_E_ARG, "npass must be in 0..8");
         if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return bfail(IMHD_E_ARG, "sound_speed and cour must be positive");
     }

@@ -302,7 +302,7 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     if (c.ny > 65535 || c.nz > 65535) return fail(IMHD_E_ARG, "ny and nz must be <= 65535");
     if (c.precision != 32 && c.precision != 64) return fail(IMHD_E_ARG, "precision must be 32 or 64");
     if (c.riemann < 1 || c.riemann > 3) return fail(IMHD_E_ARG, "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE");
-    if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) return fail(IMHD_E_ARG, "recon must be IMHD_PLM or IMHD_PPM");
+    if (c.recon < IMHD_PLM || c.recon > IMHD_PPM_PRIM) return fail(IMHD_E_ARG, "recon must be IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM");
     if (c.npass < 0 || c.npass > imhd::kMaxPass) return fail(IMHD_E_ARG, "npass must be in 0..8");
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return fail(IMHD_E_ARG, "sound_speed and cour must be positive");
     if (c.ng < 0 || c.ng_pass < 0) return fail(IMHD_E_ARG, "ghost widths must be >= 0");

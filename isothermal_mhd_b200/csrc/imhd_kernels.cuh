@@ -303,7 +303,8 @@ __device__ __forceinline__ void store_flux(T* __restrict__ F, int D, int n, int 
 template <class T, int SCHEME, int D, bool ONE>
 __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
-    constexpr bool PPM = scheme_recon(SCHEME) == 1;
+    constexpr int RECON = scheme_recon(SCHEME);
+    constexpr bool PPM = (RECON & 1) != 0, PRIM = (RECON & 2) != 0;
     int local;
     const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, D == 1 ? kSubMarchY : kSubMarchZ), local);
     Scalars* sc = rp.sc;
@@ -343,13 +344,13 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march
             load_prim<T, D>(S, dm.n, base + wrap_any(a0 - 1, na) * stride, wa, tmpbn);
             load_prim<T, D>(S, dm.n, base + a0 * stride, wb_, bnA);
             load_prim<T, D>(S, dm.n, base + wrap_up(a0, na) * stride, wc, bnB);
-            char_slope<T>(wa, wb_, wc, wc, bnA, cs, asqr, dA);
+            recon_slope<T, RECON>(wa, wb_, wc, wc, bnA, cs, asqr, dA);
             for (int a = a0; a < a1; ++a) {
                 int ap1 = wrap_up(a, na);
                 int ap2 = wrap_up(ap1, na);
                 T bnC;
                 load_prim<T, D>(S, dm.n, base + ap2 * stride, wd, bnC);
-                char_slope<T>(wb_, wc, wd, wd, bnB, cs, asqr, dB);
+                recon_slope<T, RECON>(wb_, wc, wd, wd, bnB, cs, asqr, dB);
                 T qL[7], qR[7], Fo[7];
                 plm_left_state(wb_, dA, bnA, qL);
                 plm_right_state(wc, dB, bnA, qR);
@@ -373,15 +374,15 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march
                 load_prim<T, D>(S, dm.n, base + a0 * stride, w0, bn0);
                 load_prim<T, D>(S, dm.n, base + wrap_any(a0 + 1, na) * stride, w1, bn1);
                 load_prim<T, D>(S, dm.n, base + wrap_any(a0 + 2, na) * stride, w2, bn2);
-                char_slope<T, true>(wm2, wm1, w0, w1, bnm1, cs, asqr, dm1);
-                char_slope<T, true>(wm1, w0, w1, w2, bn0, cs, asqr, d0);
-                ppm_edges(wm1, w0, w1, dm1, d0, l0, r0);
+                recon_slope<T, RECON>(wm2, wm1, w0, w1, bnm1, cs, asqr, dm1);
+                recon_slope<T, RECON>(wm1, w0, w1, w2, bn0, cs, asqr, d0);
+                ppm_edges<T, PRIM>(wm1, w0, w1, dm1, d0, l0, r0);
             }
             for (int a = a0; a < a1; ++a) {
                 load_prim<T, D>(S, dm.n, base + wrap_any(a + 3, na) * stride, w3, bn3);
-                char_slope<T, true>(w0, w1, w2, w3, bn1, cs, asqr, d1);
+                recon_slope<T, RECON>(w0, w1, w2, w3, bn1, cs, asqr, d1);
                 T l1[6], r1[6];
-                ppm_edges(w0, w1, w2, d0, d1, l1, r1);
+                ppm_edges<T, PRIM>(w0, w1, w2, d0, d1, l1, r1);
                 T qL[7], qR[7], Fo[7];
                 ppm_state(r0, bn0, qL);
                 ppm_state(l1, bn0, qR);
@@ -407,7 +408,8 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march
 template <class T, int SCHEME, int TX, bool ONE>
 __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
-    constexpr bool PPM = scheme_recon(SCHEME) == 1;
+    constexpr int RECON = scheme_recon(SCHEME);
+    constexpr bool PPM = (RECON & 1) != 0, PRIM = (RECON & 2) != 0;
     constexpr int H = PPM ? 2 : 1;           // cells staged left of the tile
     constexpr int NW = TX + (PPM ? 5 : 3);   // staged cells
     constexpr int ND = TX + (PPM ? 2 : 1);   // staged slopes, cells i0-H+1 ...
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
             wm[m] = sw[m][u]; w0[m] = sw[m][u + 1]; wp[m] = sw[m][u + 2];
             wp2[m] = PPM ? sw[m][u + 3] : sw[m][u + 2];
         }
-        char_slope<T, PPM>(wm, w0, wp, wp2, sbn[u + 1], cs, asqr, d);
+        recon_slope<T, RECON>(wm, w0, wp, wp2, sbn[u + 1], cs, asqr, d);
 #pragma unroll
         for (int m = 0; m < 6; ++m) sd[m][u] = d[m];
     }
@@ -476,8 +478,8 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
                 wm[m] = sw[m][t + 1]; w0[m] = sw[m][t + 2]; wp[m] = sw[m][t + 3]; wp2[m] = sw[m][t + 4];
                 dm1[m] = sd[m][t]; d0[m] = sd[m][t + 1]; dp[m] = sd[m][t + 2];
             }
-            ppm_edges(wm, w0, wp, dm1, d0, l, r);      // cell i
-            ppm_edges(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
+            ppm_edges<T, PRIM>(wm, w0, wp, dm1, d0, l, r);      // cell i
+            ppm_edges<T, PRIM>(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
             ppm_state(r, bn, qL);
             ppm_state(l1, bn, qR);
         }
@@ -499,7 +501,8 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
 template <class T, int SCHEME, bool ONE>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
-    constexpr bool PPM = scheme_recon(SCHEME) == 1;
+    constexpr int RECON = scheme_recon(SCHEME);
+    constexpr bool PPM = (RECON & 1) != 0, PRIM = (RECON & 2) != 0;
     extern __shared__ __align__(16) unsigned char xrow_smem[];
     int local;
     const BoxRec rp = resolve<ONE>(ba, scheme_kind(SCHEME, kSubXRow), local);
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(
             wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip];
             wp2[m] = PPM ? sw[m * nx + ip2] : wp[m];
         }
-        char_slope<T, PPM>(wm, w0, wp, wp2, sbn[i], cs, asqr, d);
+        recon_slope<T, RECON>(wm, w0, wp, wp2, sbn[i], cs, asqr, d);
 #pragma unroll
         for (int m = 0; m < 6; ++m) sd[m * nx + i] = d[m];
     }
@@ -564,8 +567,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(
                 wm[m] = sw[m * nx + im]; w0[m] = sw[m * nx + i]; wp[m] = sw[m * nx + ip]; wp2[m] = sw[m * nx + ip2];
                 dm1[m] = sd[m * nx + im]; d0[m] = sd[m * nx + i]; dp[m] = sd[m * nx + ip];
             }
-            ppm_edges(wm, w0, wp, dm1, d0, l, r);      // cell i
-            ppm_edges(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
+            ppm_edges<T, PRIM>(wm, w0, wp, dm1, d0, l, r);      // cell i
+            ppm_edges<T, PRIM>(w0, wp, wp2, d0, dp, l1, r1);    // cell i+1
             ppm_state(r, bn, qL);
             ppm_state(l1, bn, qR);
         }

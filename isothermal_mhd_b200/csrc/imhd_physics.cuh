@@ -535,8 +535,38 @@ __device__ __forceinline__ void plm_char_slope(const T* wm, const T* w0, const T
     }
 }
 
+// Primitive-variable slopes (compute_interface_states_prim, vanleer_mod.f90:
+// 1144-1485), per primitive, no eigenvectors.  PLM (:1161-1179): the MC slope
+// SIGN(1,dC) MIN(beta|dL|, beta|dR|, |dC|) with no same-sign test.  PPM
+// (:1216-1245): the MC slope with the test (mc_limit; beta MIN(|dL|,|dR|) is
+// MIN(beta|dL|, beta|dR|) exactly); what is returned is delw(i) - delw(i+1),
+// the operand of the edge formula of :1253-1254, so that ppm_edges<T, true>
+// adds sixth times it as the reference does.  wp2 = w(i+2) is read for PPM only.
+template <class T>
+__device__ __forceinline__ T prim_ppm_limit(T wm, T w0, T wp) {
+    const T dL = w0 - wm;
+    const T dR = wp - w0;
+    const T dC = T(0.5) * (dL + dR);
+    return mc_limit(dL, dR, dC);
+}
+template <class T, bool PPM>
+__device__ __forceinline__ void prim_slope(const T* wm, const T* w0, const T* wp, const T* wp2, T* delw) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        if constexpr (PPM) {
+            delw[k] = prim_ppm_limit(wm[k], w0[k], wp[k]) - prim_ppm_limit(w0[k], wp[k], wp2[k]);
+        } else {
+            const T dL = w0[k] - wm[k];
+            const T dR = wp[k] - w0[k];
+            const T dC = T(0.5) * (dL + dR);
+            delw[k] = sgn1(dC) * vmin(vmin(T(kMC_BETA) * fabs(dL), T(kMC_BETA) * fabs(dR)), fabs(dC));
+        }
+    }
+}
+
 // Interface states of face i+1/2 from the primitives and slopes of cells i
-// and i+1 (vanleer_mod.f90:1552-1584 and the prim->cons step :1799-1814).
+// and i+1 (vanleer_mod.f90:1552-1584 and the prim->cons step :1799-1814; the
+// primitive-variable PLM states of :1183-1207 are the same formulas).
 template <class T>
 __device__ __forceinline__ void plm_left_state(const T* w, const T* d, T bn, T* q) {
     q[0] = w[0] + T(0.5) * d[0];
@@ -568,21 +598,36 @@ __device__ __forceinline__ void plm_right_state(const T* w, const T* d, T bn, T*
 // left and right values from the neighbour averages and the slope
 // differences delw(i-1) (dm) and delw(i) (d0), then the monotonicity
 // constraints (flatten at an extremum, steepen an overshooting edge).
-template <class T>
+// PRIM: the primitive-variable edges of :1251-1330, where dm and d0 are the
+// slope operands of prim_slope<T, true> (added, not subtracted) and an
+// extremum flattens to the linear profile w -/+ delw(i)/2 instead of w.
+template <class T, bool PRIM = false>
 __device__ __forceinline__ void ppm_edges(const T* wm, const T* w0, const T* wp, const T* dm, const T* d0, T* wl,
                                           T* wr) {
     const T sixth = T(1.0 / 6.0);
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-        T l = T(0.5) * (wm[k] + w0[k]) - sixth * dm[k];
-        T r = T(0.5) * (w0[k] + wp[k]) - sixth * d0[k];
+        T l, r;
+        if constexpr (PRIM) {
+            l = T(0.5) * (wm[k] + w0[k]) + sixth * dm[k];
+            r = T(0.5) * (w0[k] + wp[k]) + sixth * d0[k];
+        } else {
+            l = T(0.5) * (wm[k] + w0[k]) - sixth * dm[k];
+            r = T(0.5) * (w0[k] + wp[k]) - sixth * d0[k];
+        }
         T c = w0[k];
         T tmp1 = (r - c) * (c - l);
         T tmp2 = T(6) * (r - l) * (c - T(0.5) * (l + r));
         T tmp3 = sq(r - l);
         if (tmp1 <= T(0)) {
-            l = c;
-            r = c;
+            if constexpr (PRIM) {
+                const T s = prim_ppm_limit(wm[k], w0[k], wp[k]);
+                l = c - T(0.5) * s;
+                r = c + T(0.5) * s;
+            } else {
+                l = c;
+                r = c;
+            }
         } else if (tmp2 > tmp3) {
             l = T(3) * c - T(2) * r;
         } else if (tmp2 < -tmp3) {

@@ -416,4 +416,14 @@ __device__ __forceinline__ void char_slope(const T* wm, const T* w0, const T* wp
     else plm_char_slope<T, PPM>(wm, w0, wp, wp2, bn, cs, asqr, delw);
 }
 
+// Slope of a sweep's reconstruction (scheme_recon: bit 0 PPM, bit 1 primitive
+// variables): the characteristic slope or the primitive-variable one.
+template <class T, int RECON>
+__device__ __forceinline__ void recon_slope(const T* wm, const T* w0, const T* wp, const T* wp2, T bn, T cs, T asqr,
+                                           T* delw) {
+    constexpr bool PPM = (RECON & 1) != 0;
+    if constexpr ((RECON & 2) != 0) prim_slope<T, PPM>(wm, w0, wp, wp2, delw);
+    else char_slope<T, PPM>(wm, w0, wp, wp2, bn, cs, asqr, delw);
+}
+
 }  // namespace imhd

@@ -121,7 +121,7 @@ bool valid_box(const imhd_config& c, std::string& why) {
     if (c.nx < 4 || c.ny < 4 || c.nz < 4) { why = "every edge needs at least 4 cells"; return false; }
     if ((double)c.nx * c.ny * c.nz >= 2147483647.0) { why = "box too large"; return false; }
     if (c.riemann < 1 || c.riemann > 3) { why = "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE"; return false; }
-    if (c.recon != IMHD_PLM && c.recon != IMHD_PPM) { why = "recon must be IMHD_PLM or IMHD_PPM"; return false; }
+    if (c.recon < IMHD_PLM || c.recon > IMHD_PPM_PRIM) { why = "recon must be IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM"; return false; }
     if (c.npass < 0 || c.npass > imhd::kMaxPass) { why = "npass must be in 0..8"; return false; }
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) { why = "sound_speed and cour must be positive"; return false; }
     if (c.ng < 0 || c.ng_pass < 0) { why = "ghost widths must be >= 0"; return false; }

@@ -83,7 +83,7 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
     bd.npass_max = 0;
     bd.any_zrange = false;
     for (const BoxRec& r : recs) {
-        if (r.riemann >= 1 && r.riemann <= 3 && (r.recon == 0 || r.recon == 1))
+        if (r.riemann >= 1 && r.riemann <= 3 && r.recon >= 0 && r.recon < kRecons)
             bd.has_scheme[scheme_of(r.riemann, r.recon)] = true;
         if (r.npass > 0) bd.any_pass = true;
         if (r.npass > bd.npass_max) bd.npass_max = r.npass;

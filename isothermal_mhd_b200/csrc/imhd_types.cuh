@@ -32,14 +32,17 @@ enum Kind {
     kKindCell = 0,     // (x, y) tiles of kBX threads per z plane, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
     kKindSolver0 = 2,  // + 5*(scheme-1) + {z column (predictor), x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
-    kKindCellZ = 32,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
-    kKindUpdTma = 33,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
-    kKindUpdTma64 = 34,// pairs of 64-cell row segments per z segment of it (rows of 64(2k+1) cells, even ny)
-    kKinds = 35
+    kKindCellZ = 62,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
+    kKindUpdTma = 63,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
+    kKindUpdTma64 = 64,// pairs of 64-cell row segments per z segment of it (rows of 64(2k+1) cells, even ny)
+    kKinds = 65
 };
 // A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
-// (0 PLM, 1 PPM): scheme = solver + 3 * recon, 1..kSchemes.
-constexpr int kSchemes = 6;
+// (0 PLM and 1 PPM of the characteristic variables, 2 PLM and 3 PPM of the
+// primitive variables): scheme = solver + 3 * recon, 1..kSchemes.
+constexpr int kRecons = 4;
+constexpr int kSchemes = 3 * kRecons;
+static_assert(kKindSolver0 + 5 * kSchemes == kKindCellZ, "block-decomposition kinds overlap");
 __host__ __device__ constexpr int scheme_of(int solver, int recon) { return solver + 3 * recon; }
 __host__ __device__ constexpr int scheme_solver(int scheme) { return 1 + (scheme - 1) % 3; }
 __host__ __device__ constexpr int scheme_recon(int scheme) { return (scheme - 1) / 3; }
@@ -79,7 +82,7 @@ struct Scalars {
 struct BoxRec {
     int nx, ny, nz, n;
     int npass, riemann, plane_stride, nred;
-    int active, recon;      // running flag; 0 PLM, 1 PPM
+    int active, recon;      // running flag; 0 PLM, 1 PPM (characteristic), 2 PLM, 3 PPM (primitive)
     int zlo, zhi;           // z planes whose cells and faces enter the step's maxima and sums
     int tws, pad2_;         // x width of the cell tiles is 1 << tws (32, 64 or 128), height kBX >> tws
     int segs, segzs;        // faces per thread of the y / z sweeps 1 << segs; segzs == kSegZLog (reserved)

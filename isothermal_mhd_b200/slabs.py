@@ -45,7 +45,7 @@ import numpy as np
 
 def halo_width(recon="plm", npass=0):
     """Halo planes a slab needs for one exact step."""
-    r = 6 if recon == "ppm" else 5
+    r = 6 if recon in ("ppm", "ppm-prim") else 5
     return r + (1 if npass else 0)
 
 

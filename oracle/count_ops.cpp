@@ -77,10 +77,11 @@ extern "C" {
 
 // Same layout and meaning as oracle_create / oracle_set_state in
 // imhd_oracle_capi.cpp; one host thread (the tally is not synchronised).
-void* ops_create(int nx, int ny, int nz, int riemann, int ppm, int npass, double sound_speed) {
+void* ops_create(int nx, int ny, int nz, int riemann, int recon, int npass, double sound_speed) {
     Config c;
     c.nx = nx; c.ny = ny; c.nz = nz;
-    c.riemann = riemann; c.ppm = ppm; c.npass = npass;
+    c.riemann = riemann; c.ppm = recon & 1; c.prim = (recon >> 1) & 1; c.protect = (recon >> 2) & 1;
+    c.npass = npass;
     c.sound_speed = sound_speed; c.nthreads = 1;
     c.nb = 6;
     if (nx < 2 * c.nb || ny < 2 * c.nb || nz < 2 * c.nb) return nullptr;

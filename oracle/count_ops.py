@@ -66,7 +66,8 @@ def tally_step(n, riemann, recon, npass, seed=20261203):
     from isothermal_mhd_b200 import forcing
     q, b, p = forcing.turbulent_box(n, mach=2.0, b0=(0.5, 0.0, 0.0), npass=npass, seed=seed)
     L = lib()
-    h = L.ops_create(n, n, n, {"roe": 1, "hlld": 2, "hlle": 3}[riemann], 1 if recon == "ppm" else 0, npass, 1.0)
+    code = {"plm": 0, "ppm": 1, "plm-prim": 2, "ppm-prim": 3}[recon]
+    h = L.ops_create(n, n, n, {"roe": 1, "hlld": 2, "hlle": 3}[riemann], code, npass, 1.0)
     try:
         q, b = np.ascontiguousarray(q), np.ascontiguousarray(b)
         p = np.ascontiguousarray(p) if npass else None

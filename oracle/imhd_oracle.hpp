@@ -41,8 +41,10 @@
 //  * generate_rand_force reads entries of delvk_re/im that the reference never
 //    assigns (mixed-sign wave vectors); here they are defined as 0.
 //  * The optional HLLE "flux protection" and the primitive-variable
-//    reconstruction are switched off in the reference (vanleer_mod.f90:81,84)
-//    and are not restated.
+//    reconstruction are switched off in the reference (vanleer_mod.f90:81,84);
+//    both are restated behind Config::protect and Config::prim.  Protection is
+//    restated for the Roe solver only: the reference computes its protection
+//    fluxes in the Roe branch alone (:540, 703, 880).
 //  * Arrays are padded exactly like the reference (nb ghost layers, nb-2 for the
 //    passive scalars) and every loop runs over the same ranges, so ghost-region
 //    work is reproduced too.
@@ -78,6 +80,8 @@ struct Config {
     double sound_speed = 1.0;   // constants_mod.f90:35
     int riemann = 1;            // 1 Roe, 2 HLLD, 3 HLLE (constants_mod.f90:57)
     int ppm = 0;                // 0 PLM (the benchmarked path), 1 PPM (reference default)
+    int prim = 0;               // 1: primitive-variable reconstruction (primitive_reconstruction, vanleer_mod.f90:84)
+    int protect = 0;            // 1: HLLE protection fluxes for bad cells (flux_protection, vanleer_mod.f90:81)
     int npass = 0;              // passive scalars (constants_mod.f90:63)
     double edot = 1.0e-3;       // constants_mod.f90:44
     double dt_turb = 0.05;      // constants_mod.f90:42
@@ -129,7 +133,7 @@ static const int EMF_POS[3][3] = {{2, 1, 7}, {3, 2, 5}, {1, 2, 6}};
 
 struct Work {
     // MHD sweep work arrays (vanleer_mod.f90:88-110, 179-194)
-    Arr2 qintL, qintR, w, wb, Rw, Lw, wL, wR, delw, Fs2d;
+    Arr2 qintL, qintR, w, wb, Rw, Lw, wL, wR, delw, Fs2d, Fs2dp;
     Arr2 qavg, Rk, ck, eig, ws, alphaf, alphas, betay, betaz, F, FTVD;
     // passive sweep work arrays (passive_mod.f90:23-30)
     Arr2 p_int, p_w, p_F, p_vel, p_delw;
@@ -142,6 +146,10 @@ public:
     int nx, ny, nz, nb, nmax, nbp = 3;
     double dx, dt = 0.0, smax = 0.0, delv_max = 0.0, asqr, cs;
     Arr q, bface, emf_corner, qpass, qwork, bface_work, Fs, emf3d;
+    // flux protection (vanleer_mod.f90:81, 88-110): HLLE fluxes and EMFs of
+    // the same interface states, the state before an update, the bad cells
+    Arr Fs_prot, emf3d_prot, emf_corner_prot, q_prot;
+    std::vector<char> prot_flags;
     Arr qpass_work, Fpass, vel, vel_tavg;
     Arr delv, rho0;
     bool have_force = false;
@@ -167,6 +175,13 @@ public:
         Fs.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 21);
         emf3d.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 9);
         rho0.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 1);
+        if (c.protect) {
+            Fs_prot.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 21);
+            emf3d_prot.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 9);
+            emf_corner_prot.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 3);
+            q_prot.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 7);
+            prot_flags.assign(q_prot.d.size() / 7, 0);
+        }
         delv.init(1 - nb, nx + nb, 1 - nb, ny + nb, 1 - nb, nz + nb, 3);
         if (c.npass > 0) {
             qpass.init(1 - nb + 2, nx + nb - 2, 1 - nb + 2, ny + nb - 2, 1 - nb + 2, nz + nb - 2, c.npass);
@@ -183,6 +198,7 @@ public:
             wk.Rw.init(lo, hi, 36); wk.Lw.init(lo, hi, 36);
             wk.wL.init(lo, hi, 6); wk.wR.init(lo, hi, 6); wk.delw.init(lo, hi, 6);
             wk.Fs2d.init(lo, hi, 7);
+            if (c.protect) wk.Fs2dp.init(lo, hi, 7);
             wk.qavg.init(lo, hi, 7); wk.Rk.init(lo, hi, 36); wk.ck.init(lo, hi, 6);
             wk.eig.init(lo, hi, 6); wk.ws.init(lo, hi, 3);
             wk.alphaf.init(lo, hi, 1); wk.alphas.init(lo, hi, 1);
@@ -297,6 +313,7 @@ public:
         Fs.fill(0.0);
         emf3d.fill(0.0);
         emf_corner.fill(0.0);
+        if (protecting()) Fs_prot.fill(0.0);
         smax = 0.0;
         delv_max = 0.0;
         if (drive_next) get_rho_turb();
@@ -304,7 +321,8 @@ public:
         int off = 0;
         for (int d = 0; d < 3; ++d) compute_fluxes_3d(d, 1 + off, false);
         compute_cell_center_emf_3d(1 + off);
-        compute_cell_corner_emf_3d(1 + off);
+        compute_cell_corner_emf_3d(1 + off, emf3d, emf_corner);
+        if (protecting()) compute_cell_corner_emf_3d(1 + off, emf3d_prot, emf_corner_prot);
         double dtdx = 0.5 * dt / dx;
         update_hydro_state_3d(dtdx, 1 + off);
         update_CT_3d(dtdx, 1 + off);
@@ -313,7 +331,8 @@ public:
         for (int d = 0; d < 3; ++d) compute_fluxes_3d(d, 1 + off, true);
         off = cfg.ppm ? 4 : 3;
         compute_cell_center_emf_3d(1 + off);
-        compute_cell_corner_emf_3d(1 + off);
+        compute_cell_corner_emf_3d(1 + off, emf3d, emf_corner);
+        if (protecting()) compute_cell_corner_emf_3d(1 + off, emf3d_prot, emf_corner_prot);
 
         q.d = qwork.d;
         bface.d = bface_work.d;
@@ -323,6 +342,10 @@ public:
 
         if (drive_next) add_random_force();
     }
+
+    // flux protection is restated for the Roe solver (the only one whose
+    // branch computes protection fluxes, vanleer_mod.f90:540, 703, 880)
+    bool protecting() const { return cfg.protect && cfg.riemann == 1; }
 
     // cell (i,j,k) of along/transverse/plane indices (a,b,p) for sweep d
     inline void cell(int d, long a, long b, long p, long& i, long& j, long& k) const {
@@ -383,8 +406,12 @@ public:
                         wk.w(a, b, 5) = q(i, j, k, btr[0]);
                         wk.w(a, b, 6) = q(i, j, k, btr[1]);
                     }
-                compute_primitive_eigenvectors(wk, alo, ahi, blo, bhi);
-                compute_interface_states_char(wk, alo, ahi, blo, bhi);
+                if (cfg.prim) {
+                    compute_interface_states_prim(wk, alo, ahi, blo, bhi);
+                } else {
+                    compute_primitive_eigenvectors(wk, alo, ahi, blo, bhi);
+                    compute_interface_states_char(wk, alo, ahi, blo, bhi);
+                }
                 offset = cfg.ppm ? 2 : 1;
             }
 
@@ -397,6 +424,7 @@ public:
                 compute_roe_eigenvalues_1d(wk, alo + offset, ahi - offset, blo, bhi);
                 compute_roe_eigenvectors_1d(wk, alo + offset, ahi - offset, blo, bhi);
                 compute_ROE_fluxes_1d(wk, alo + offset, ahi - offset, blo, bhi);
+                if (protecting()) compute_HLLE_fluxes_1d(wk, alo + offset, ahi - offset, blo, bhi, true);
             }
 
             for (long b = blo - nb; b <= bhi + nb; ++b)
@@ -405,6 +433,11 @@ public:
                     for (int r = 1; r <= 7; ++r) Fs(i, j, k, SCAT[d][r - 1] + 7 * d) = wk.Fs2d(a, b, r);
                     emf3d(i, j, k, EMF_NEG[d][0] + 3 * (EMF_NEG[d][1] - 1)) = -Fs(i, j, k, EMF_NEG[d][2] + 7 * d);
                     emf3d(i, j, k, EMF_POS[d][0] + 3 * (EMF_POS[d][1] - 1)) = Fs(i, j, k, EMF_POS[d][2] + 7 * d);
+                    if (protecting()) {
+                        for (int r = 1; r <= 7; ++r) Fs_prot(i, j, k, SCAT[d][r - 1] + 7 * d) = wk.Fs2dp(a, b, r);
+                        emf3d_prot(i, j, k, EMF_NEG[d][0] + 3 * (EMF_NEG[d][1] - 1)) = -Fs_prot(i, j, k, EMF_NEG[d][2] + 7 * d);
+                        emf3d_prot(i, j, k, EMF_POS[d][0] + 3 * (EMF_POS[d][1] - 1)) = Fs_prot(i, j, k, EMF_POS[d][2] + 7 * d);
+                    }
                 }
         });
         reduce_smax();
@@ -623,6 +656,114 @@ public:
                         if (tmp1 <= 0.0) {
                             wk.wL(i, j, k) = wc;
                             wk.wR(i, j, k) = wc;
+                        } else if (tmp2 > tmp3) {
+                            wk.wL(i, j, k) = 3.0 * wc - 2.0 * wr;
+                        } else if (tmp2 < -tmp3) {
+                            wk.wR(i, j, k) = 3.0 * wc - 2.0 * wl;
+                        }
+                    }
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 2; i <= ihi + nb - 3; ++i) {
+                    wk.qintL(i, j, 1) = wk.wR(i, j, 1);
+                    wk.qintL(i, j, 2) = wk.wR(i, j, 2);
+                    wk.qintL(i, j, 3) = wk.wR(i, j, 3);
+                    wk.qintL(i, j, 4) = wk.wR(i, j, 4);
+                    wk.qintL(i, j, 5) = wk.wb(i, j, 1);
+                    wk.qintL(i, j, 6) = wk.wR(i, j, 5);
+                    wk.qintL(i, j, 7) = wk.wR(i, j, 6);
+                    wk.qintR(i, j, 1) = wk.wL(i + 1, j, 1);
+                    wk.qintR(i, j, 2) = wk.wL(i + 1, j, 2);
+                    wk.qintR(i, j, 3) = wk.wL(i + 1, j, 3);
+                    wk.qintR(i, j, 4) = wk.wL(i + 1, j, 4);
+                    wk.qintR(i, j, 5) = wk.wb(i, j, 1);
+                    wk.qintR(i, j, 6) = wk.wL(i + 1, j, 5);
+                    wk.qintR(i, j, 7) = wk.wL(i + 1, j, 6);
+                }
+            offset = 1;
+        }
+        for (long j = jlow - nb; j <= jhi + nb; ++j)
+            for (long i = ilow - nb + 1 + offset; i <= ihi + nb - 2 - offset; ++i) {
+                wk.qintL(i, j, 2) = wk.qintL(i, j, 2) * wk.qintL(i, j, 1);
+                wk.qintL(i, j, 3) = wk.qintL(i, j, 3) * wk.qintL(i, j, 1);
+                wk.qintL(i, j, 4) = wk.qintL(i, j, 4) * wk.qintL(i, j, 1);
+                wk.qintR(i, j, 2) = wk.qintR(i, j, 2) * wk.qintR(i, j, 1);
+                wk.qintR(i, j, 3) = wk.qintR(i, j, 3) * wk.qintR(i, j, 1);
+                wk.qintR(i, j, 4) = wk.qintR(i, j, 4) * wk.qintR(i, j, 1);
+            }
+    }
+
+    // vanleer_mod.f90:1144-1485 (primitive-variable reconstruction).  PLM
+    // (:1161-1212): the MC slope of each primitive without a same-sign test,
+    // SIGN(1,dC)*MIN(beta|dL|, beta|dR|, |dC|).  PPM (:1214-1431): MC slopes
+    // with the same-sign test, parabolic edges from the neighbour averages and
+    // the slope differences, the monotonicity constraints (an extremum
+    // flattens to the linear profile w -/+ delw/2); the discontinuity
+    // steepener is off (:86) and the block after it is skipped by its
+    // GO TO 1000 (:1336).  Then prim->cons (:1460-1482).
+    void compute_interface_states_prim(Work& wk, long ilow, long ihi, long jlow, long jhi) {
+        const double sixth = 1.0 / 6.0;
+        int offset;
+        if (!cfg.ppm) {
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 1; i <= ihi + nb - 1; ++i)
+                    for (int k = 1; k <= 6; ++k) {
+                        double dL = wk.w(i, j, k) - wk.w(i - 1, j, k);
+                        double dR = wk.w(i + 1, j, k) - wk.w(i, j, k);
+                        double dC = 0.5 * (dL + dR);
+                        wk.delw(i, j, k) = fsign(1.0, dC) * fmin3(MC_BETA * std::fabs(dL), MC_BETA * std::fabs(dR),
+                                                                   std::fabs(dC));
+                    }
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 1; i <= ihi + nb - 2; ++i) {
+                    wk.qintL(i, j, 1) = wk.w(i, j, 1) + 0.5 * wk.delw(i, j, 1);
+                    wk.qintL(i, j, 2) = wk.w(i, j, 2) + 0.5 * wk.delw(i, j, 2);
+                    wk.qintL(i, j, 3) = wk.w(i, j, 3) + 0.5 * wk.delw(i, j, 3);
+                    wk.qintL(i, j, 4) = wk.w(i, j, 4) + 0.5 * wk.delw(i, j, 4);
+                    wk.qintL(i, j, 5) = wk.wb(i, j, 1);
+                    wk.qintL(i, j, 6) = wk.w(i, j, 5) + 0.5 * wk.delw(i, j, 5);
+                    wk.qintL(i, j, 7) = wk.w(i, j, 6) + 0.5 * wk.delw(i, j, 6);
+                }
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 1; i <= ihi + nb - 2; ++i) {
+                    wk.qintR(i, j, 1) = wk.w(i + 1, j, 1) - 0.5 * wk.delw(i + 1, j, 1);
+                    wk.qintR(i, j, 2) = wk.w(i + 1, j, 2) - 0.5 * wk.delw(i + 1, j, 2);
+                    wk.qintR(i, j, 3) = wk.w(i + 1, j, 3) - 0.5 * wk.delw(i + 1, j, 3);
+                    wk.qintR(i, j, 4) = wk.w(i + 1, j, 4) - 0.5 * wk.delw(i + 1, j, 4);
+                    wk.qintR(i, j, 5) = wk.wb(i, j, 1);
+                    wk.qintR(i, j, 6) = wk.w(i + 1, j, 5) - 0.5 * wk.delw(i + 1, j, 5);
+                    wk.qintR(i, j, 7) = wk.w(i + 1, j, 6) - 0.5 * wk.delw(i + 1, j, 6);
+                }
+            offset = 0;
+        } else {
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 1; i <= ihi + nb - 1; ++i)
+                    for (int k = 1; k <= 6; ++k) {
+                        double dL = wk.w(i, j, k) - wk.w(i - 1, j, k);
+                        double dR = wk.w(i + 1, j, k) - wk.w(i, j, k);
+                        double dC = 0.5 * (dL + dR);
+                        double lim = 0.0;
+                        double mabs = fmin2(std::fabs(dL), std::fabs(dR));
+                        if ((dL * dR) > 0.0) lim = fsign(1.0, dC) * fmin2(MC_BETA * mabs, std::fabs(dC));
+                        wk.delw(i, j, k) = lim;
+                    }
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 2; i <= ihi + nb - 2; ++i)
+                    for (int k = 1; k <= 6; ++k) {
+                        wk.wL(i, j, k) = 0.5 * (wk.w(i - 1, j, k) + wk.w(i, j, k)) +
+                                         sixth * (wk.delw(i - 1, j, k) - wk.delw(i, j, k));
+                        wk.wR(i, j, k) = 0.5 * (wk.w(i, j, k) + wk.w(i + 1, j, k)) +
+                                         sixth * (wk.delw(i, j, k) - wk.delw(i + 1, j, k));
+                    }
+            for (long j = jlow - nb; j <= jhi + nb; ++j)
+                for (long i = ilow - nb + 2; i <= ihi + nb - 2; ++i)
+                    for (int k = 1; k <= 6; ++k) {
+                        double wc = wk.w(i, j, k), wl = wk.wL(i, j, k), wr = wk.wR(i, j, k);
+                        double tmp1 = (wr - wc) * (wc - wl);
+                        double tmp2 = 6.0 * (wr - wl) * (wc - 0.5 * (wl + wr));
+                        double tmp3 = sq(wr - wl);
+                        if (tmp1 <= 0.0) {
+                            wk.wL(i, j, k) = wc - 0.5 * wk.delw(i, j, k);
+                            wk.wR(i, j, k) = wc + 0.5 * wk.delw(i, j, k);
                         } else if (tmp2 > tmp3) {
                             wk.wL(i, j, k) = 3.0 * wc - 2.0 * wr;
                         } else if (tmp2 < -tmp3) {
@@ -936,7 +1077,9 @@ public:
     }
 
     // vanleer_mod.f90:2867-2981
-    void compute_HLLE_fluxes_1d(Work& wk, long ilow, long ihi, long jlow, long jhi) {
+    // prot: into the protection flux buffer (vanleer_mod.f90:540)
+    void compute_HLLE_fluxes_1d(Work& wk, long ilow, long ihi, long jlow, long jhi, bool prot = false) {
+        Arr2& Fout = prot ? wk.Fs2dp : wk.Fs2d;
         for (long j = jlow - nb; j <= jhi + nb; ++j)
             for (long i = ilow - nb; i <= ihi + nb - 1; ++i) {
                 double uL[7], uR[7], ua[7], FL[7], FR[7];
@@ -958,7 +1101,7 @@ public:
                 wk.smax = fmax4(wk.smax, std::fabs(vxL) + cfL, std::fabs(vxR) + cfR, std::fabs(vxa) + cfa);
                 double isRL = 1.0 / (sR - sL);
                 for (int m = 0; m < 7; ++m)
-                    wk.Fs2d(i, j, m + 1) = (sR * FL[m] - sL * FR[m] + sR * sL * (uR[m] - uL[m])) * isRL;
+                    Fout(i, j, m + 1) = (sR * FL[m] - sL * FR[m] + sR * sL * (uR[m] - uL[m])) * isRL;
             }
     }
 
@@ -1059,13 +1202,16 @@ public:
                     emf3d(i, j, k, 1 + 6) = (q(i, j, k, 6) * q(i, j, k, 4) - q(i, j, k, 7) * q(i, j, k, 3)) * irho;
                     emf3d(i, j, k, 2 + 6) = (q(i, j, k, 7) * q(i, j, k, 2) - q(i, j, k, 5) * q(i, j, k, 4)) * irho;
                     emf3d(i, j, k, 3 + 6) = (q(i, j, k, 5) * q(i, j, k, 3) - q(i, j, k, 6) * q(i, j, k, 2)) * irho;
+                    if (protecting())
+                        for (int c = 1; c <= 3; ++c) emf3d_prot(i, j, k, c + 6) = emf3d(i, j, k, c + 6);
                 }
         });
     }
-    inline double E(long i, long j, long k, int c, int s) { return emf3d(i, j, k, c + 3 * (s - 1)); }
 
-    // vanleer_mod.f90:1884-2076
-    void compute_cell_corner_emf_3d(int lo) {
+    // vanleer_mod.f90:1884-2076, from the face and cell-centre EMFs em into
+    // the corner EMFs ec (emf_3d -> emf_corner, or the protection pair)
+    void compute_cell_corner_emf_3d(int lo, Arr& em, Arr& ec) {
+        auto E = [&em](long i, long j, long k, int c, int s) { return em(i, j, k, c + 3 * (s - 1)); };
         long ilo = lo, ihi = nx - (lo - 1), jlo = lo, jhi = ny - (lo - 1), klo = lo, khi = nz - (lo - 1);
         parallel_for(klo - nb, khi + nb - 1, [&](long k, int) {
             for (long j = jlo - nb; j <= jhi + nb - 1; ++j)
@@ -1088,7 +1234,7 @@ public:
                     if (vy > ZERO) { dx1412 = dxL14; dx3412 = dxL34; }
                     else if (vy < -ZERO) { dx1412 = dxR14; dx3412 = dxR34; }
                     else { dx1412 = 0.5 * (dxL14 + dxR14); dx3412 = 0.5 * (dxL34 + dxR34); }
-                    emf_corner(i, j, k, 3) = 0.25 * (E(i, j, k, 3, 1) + E(i, j + 1, k, 3, 1) + E(i, j, k, 3, 2) + E(i + 1, j, k, 3, 2)) +
+                    ec(i, j, k, 3) = 0.25 * (E(i, j, k, 3, 1) + E(i, j + 1, k, 3, 1) + E(i, j, k, 3, 2) + E(i + 1, j, k, 3, 2)) +
                                              0.125 * ((dy1214 - dy1234) + (dx1412 - dx3412));
                 }
         });
@@ -1113,7 +1259,7 @@ public:
                     if (vz > ZERO) { dx1412 = dxL14; dx3412 = dxL34; }
                     else if (vz < -ZERO) { dx1412 = dxR14; dx3412 = dxR34; }
                     else { dx1412 = 0.5 * (dxL14 + dxR14); dx3412 = 0.5 * (dxL34 + dxR34); }
-                    emf_corner(i, j, k, 2) = 0.25 * (E(i, j, k, 2, 1) + E(i, j, k + 1, 2, 1) + E(i, j, k, 2, 2) + E(i + 1, j, k, 2, 2)) +
+                    ec(i, j, k, 2) = 0.25 * (E(i, j, k, 2, 1) + E(i, j, k + 1, 2, 1) + E(i, j, k, 2, 2) + E(i + 1, j, k, 2, 2)) +
                                              0.125 * ((dz1214 - dz1234) + (dx1412 - dx3412));
                 }
         });
@@ -1138,16 +1284,30 @@ public:
                     if (vz > ZERO) { dy1412 = dyL14; dy3412 = dyL34; }
                     else if (vz < -ZERO) { dy1412 = dyR14; dy3412 = dyR34; }
                     else { dy1412 = 0.5 * (dyL14 + dyR14); dy3412 = 0.5 * (dyL34 + dyR34); }
-                    emf_corner(i, j, k, 1) = 0.25 * (E(i, j, k, 1, 1) + E(i, j, k + 1, 1, 1) + E(i, j, k, 1, 2) + E(i, j + 1, k, 1, 2)) +
+                    ec(i, j, k, 1) = 0.25 * (E(i, j, k, 1, 1) + E(i, j, k + 1, 1, 1) + E(i, j, k, 1, 2) + E(i, j + 1, k, 1, 2)) +
                                              0.125 * ((dz1214 - dz1234) + (dy1412 - dy3412));
                 }
         });
     }
 
-    // vanleer_mod.f90:2080-2207 (protection branch off) + :3243-3262
+    // vanleer_mod.f90:2080-2207 + :3243-3262.  With protection: after the
+    // update, every cell whose density fell below MIN_DENS takes the
+    // protection fluxes on its six faces and the protection corner EMFs at
+    // (i,j,k), (i-1,j,k), (i,j-1,k), (i,j,k-1) of each component (the set the
+    // reference copies, :2147-2171), and the bad cells and their six
+    // neighbours are updated again from the state before the update (:2179-2201).
     long floor_hits = 0;
+    long prot_cells = 0;     // interior bad cells of all protected updates so far
+    size_t pidx(long i, long j, long k) const {
+        return (size_t)((i - q_prot.lo0) + q_prot.n0 * ((j - q_prot.lo1) + q_prot.n1 * (k - q_prot.lo2)));
+    }
     void update_hydro_state_3d(double dtdx, int lo) {
         long ilo = lo, ihi = nx - (lo - 1), jlo = lo, jhi = ny - (lo - 1), klo = lo, khi = nz - (lo - 1);
+        const bool prot = protecting();
+        if (prot) {
+            std::fill(prot_flags.begin(), prot_flags.end(), 0);
+            q_prot.d = q.d;
+        }
         parallel_for(klo - nb + 1, khi + nb - 1, [&](long k, int) {
             for (long j = jlo - nb + 1; j <= jhi + nb - 1; ++j)
                 for (long i = ilo - nb + 1; i <= ihi + nb - 1; ++i)
@@ -1156,6 +1316,43 @@ public:
                                                                 (Fs(i, j, k, v + 7) - Fs(i, j - 1, k, v + 7)) +
                                                                 (Fs(i, j, k, v + 14) - Fs(i, j, k - 1, v + 14)));
         });
+        if (prot) {
+            long bad = 0;
+            for (long k = klo - nb + 1; k <= khi + nb - 1; ++k)
+                for (long j = jlo - nb + 1; j <= jhi + nb - 1; ++j)
+                    for (long i = ilo - nb + 1; i <= ihi + nb - 1; ++i)
+                        if (q(i, j, k, 1) < MIN_DENS) {
+                            prot_flags[pidx(i, j, k)] = 1;
+                            if (i >= 1 && i <= nx && j >= 1 && j <= ny && k >= 1 && k <= nz) ++bad;
+                            for (int v = 1; v <= 7; ++v) {
+                                Fs(i, j, k, v) = Fs_prot(i, j, k, v);
+                                Fs(i - 1, j, k, v) = Fs_prot(i - 1, j, k, v);
+                                Fs(i, j, k, v + 7) = Fs_prot(i, j, k, v + 7);
+                                Fs(i, j - 1, k, v + 7) = Fs_prot(i, j - 1, k, v + 7);
+                                Fs(i, j, k, v + 14) = Fs_prot(i, j, k, v + 14);
+                                Fs(i, j, k - 1, v + 14) = Fs_prot(i, j, k - 1, v + 14);
+                            }
+                            for (int c = 1; c <= 3; ++c) {
+                                emf_corner(i, j, k, c) = emf_corner_prot(i, j, k, c);
+                                emf_corner(i - 1, j, k, c) = emf_corner_prot(i - 1, j, k, c);
+                                emf_corner(i, j - 1, k, c) = emf_corner_prot(i, j - 1, k, c);
+                                emf_corner(i, j, k - 1, c) = emf_corner_prot(i, j, k - 1, c);
+                            }
+                        }
+            prot_cells += bad;
+            for (long k = klo - nb + 1; k <= khi + nb - 1; ++k)
+                for (long j = jlo - nb + 1; j <= jhi + nb - 1; ++j)
+                    for (long i = ilo - nb + 1; i <= ihi + nb - 1; ++i) {
+                        if (!(prot_flags[pidx(i, j, k)] || prot_flags[pidx(i - 1, j, k)] || prot_flags[pidx(i + 1, j, k)] ||
+                              prot_flags[pidx(i, j - 1, k)] || prot_flags[pidx(i, j + 1, k)] ||
+                              prot_flags[pidx(i, j, k - 1)] || prot_flags[pidx(i, j, k + 1)]))
+                            continue;
+                        for (int v = 1; v <= 4; ++v)
+                            q(i, j, k, v) = q_prot(i, j, k, v) - dtdx * ((Fs(i, j, k, v) - Fs(i - 1, j, k, v)) +
+                                                                         (Fs(i, j, k, v + 7) - Fs(i, j - 1, k, v + 7)) +
+                                                                         (Fs(i, j, k, v + 14) - Fs(i, j, k - 1, v + 14)));
+                    }
+        }
         for (long k = klo - nb + 1; k <= khi + nb - 1; ++k)
             for (long j = jlo - nb + 1; j <= jhi + nb - 1; ++j)
                 for (long i = ilo - nb + 1; i <= ihi + nb - 1; ++i)

@@ -15,10 +15,13 @@ using imhd_oracle::Solver;
 
 extern "C" {
 
-void* oracle_create(int nx, int ny, int nz, int riemann, int ppm, int npass, double sound_speed, int nthreads) {
+// recon: bit 0 PPM (else PLM), bit 1 primitive-variable (else characteristic)
+// reconstruction; bit 2 the HLLE protection fluxes of a Roe run.
+void* oracle_create(int nx, int ny, int nz, int riemann, int recon, int npass, double sound_speed, int nthreads) {
     Config c;
     c.nx = nx; c.ny = ny; c.nz = nz;
-    c.riemann = riemann; c.ppm = ppm; c.npass = npass;
+    c.riemann = riemann; c.ppm = recon & 1; c.prim = (recon >> 1) & 1; c.protect = (recon >> 2) & 1;
+    c.npass = npass;
     c.sound_speed = sound_speed; c.nthreads = nthreads;
     c.nb = 6;
     if (nx < 2 * c.nb || ny < 2 * c.nb || nz < 2 * c.nb) return nullptr;
@@ -96,6 +99,7 @@ double oracle_smax(void* h) { return static_cast<Solver*>(h)->smax; }
 double oracle_delv_max(void* h) { return static_cast<Solver*>(h)->delv_max; }
 double oracle_dx(void* h) { return static_cast<Solver*>(h)->dx; }
 long oracle_floor_hits(void* h) { return static_cast<Solver*>(h)->floor_hits; }
+long oracle_prot_cells(void* h) { return static_cast<Solver*>(h)->prot_cells; }
 int oracle_force_error(void* h) { return static_cast<Solver*>(h)->force_error; }
 
 // out = {KE, vrms, momx, momy, momz, divB} (driver.f90:492-553)

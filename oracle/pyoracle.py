@@ -54,6 +54,8 @@ def lib():
             getattr(L, name).argtypes = [vp]
         L.oracle_floor_hits.restype = ctypes.c_long
         L.oracle_floor_hits.argtypes = [vp]
+        L.oracle_prot_cells.restype = ctypes.c_long
+        L.oracle_prot_cells.argtypes = [vp]
         L.oracle_force_error.restype = i
         L.oracle_force_error.argtypes = [vp]
         L.oracle_diagnostics.argtypes = [vp, dp]
@@ -68,16 +70,25 @@ def _ptr(a):
 
 
 RIEMANN = {"roe": 1, "hlld": 2, "hlle": 3}
+# reconstruction code of oracle_create: bit 0 PPM, bit 1 primitive variables
+RECON = {"plm": 0, "ppm": 1, "plm-prim": 2, "ppm-prim": 3}
+
+
+def recon_code(recon, protect=False):
+    return RECON[recon] | (4 if protect else 0)
 
 
 class Oracle:
     """One periodic box advanced by the CPU restatement of the reference."""
 
-    def __init__(self, n, riemann="roe", recon="plm", npass=0, sound_speed=1.0, nthreads=1):
+    def __init__(self, n, riemann="roe", recon="plm", npass=0, sound_speed=1.0, nthreads=1, protect=False):
+        """recon: "plm" / "ppm" characteristic (the reference default) or
+        "plm-prim" / "ppm-prim" primitive-variable reconstruction; protect:
+        the HLLE protection fluxes of a Roe run (flux_protection)."""
         nx, ny, nz = (n, n, n) if np.isscalar(n) else n
         self.shape = (nz, ny, nx)
         self.npass = npass
-        self.h = lib().oracle_create(nx, ny, nz, RIEMANN[riemann], 1 if recon == "ppm" else 0,
+        self.h = lib().oracle_create(nx, ny, nz, RIEMANN[riemann], recon_code(recon, protect),
                                      npass, float(sound_speed), int(nthreads))
         if not self.h:
             raise ValueError("oracle needs every edge >= 12 cells (nb = 6 ghost layers)")
@@ -148,6 +159,11 @@ class Oracle:
     @property
     def floor_hits(self):
         return lib().oracle_floor_hits(self.h)
+
+    @property
+    def prot_cells(self):
+        """Interior cells the protection re-updated (counted per update)."""
+        return lib().oracle_prot_cells(self.h)
 
     @property
     def force_error(self):
