@@ -60,6 +60,7 @@ extern "C" {
 #define IMHD_S_ZERO_SPEED 4u/* max speed < 1e-20 (vanleer_mod.f90:3328) */
 #define IMHD_S_FORCE 8u     /* forcing quadratic term <= 1e-20 (turb_driver_mod.f90:420) */
 #define IMHD_S_WAIT 16u     /* a bounded wait for an asynchronous copy in a kernel gave up; the step is not valid */
+#define IMHD_S_PROTECT 32u  /* flux protection found more bad cells than its list holds (2^20 per update); the step is not valid */
 
 typedef struct imhd_config {
     int nx, ny, nz;        /* interior cells per axis (constants_mod.f90:9-11) */
@@ -74,6 +75,11 @@ typedef struct imhd_config {
     int ng;                /* ghost layers of host q / bface / delv arrays */
     int ng_pass;           /* ghost layers of host qpass arrays */
     int device;            /* CUDA device ordinal */
+    int protect;           /* 1: flux_protection (vanleer_mod.f90:81, off in the reference) for an IMHD_ROE box: HLLE
+                            * fluxes of the same interface states are kept beside the Roe fluxes (their wave speeds
+                            * enter smax, :2962), and after each update the cells whose density fell below 1e-20 and
+                            * their six neighbours are updated again with the HLLE fluxes on the bad cells' faces and
+                            * the HLLE corner EMFs (:2086-2202); needs 21 more fields of device memory */
 } imhd_config;
 
 typedef struct imhd_box imhd_box;

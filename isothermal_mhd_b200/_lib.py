@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libimhd.so")
 IMHD_OK = 0
 IMHD_E_PHYSICS = 4
 ERRORS = {1: "IMHD_E_ARG", 2: "IMHD_E_CUDA", 3: "IMHD_E_NOMEM", 4: "IMHD_E_PHYSICS", 5: "IMHD_E_STATE"}
-S_FLOOR, S_NAN, S_ZERO_SPEED, S_FORCE = 1, 2, 4, 8
+S_FLOOR, S_NAN, S_ZERO_SPEED, S_FORCE, S_WAIT, S_PROTECT = 1, 2, 4, 8, 16, 32
 # interface reconstruction (imhd_config.recon): characteristic PLM / PPM (the
 # reference's default, vanleer_mod.f90:1488-1818) or primitive-variable PLM / PPM
 # (primitive_reconstruction, :1144-1485)
@@ -49,6 +49,7 @@ class ImhdConfig(ctypes.Structure):
         ("sound_speed", ctypes.c_double), ("cour", ctypes.c_double),
         ("edot", ctypes.c_double), ("dt_turb", ctypes.c_double),
         ("ng", ctypes.c_int), ("ng_pass", ctypes.c_int), ("device", ctypes.c_int),
+        ("protect", ctypes.c_int),
     ]
 
 

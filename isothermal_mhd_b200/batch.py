@@ -17,7 +17,7 @@ from .box import RIEMANN, _dptr
 
 
 def make_config(n, precision=32, riemann="roe", npass=0, sound_speed=1.0, cour=0.4, edot=0.0, dt_turb=0.05,
-                ng=0, ng_pass=None, device=0, recon="plm"):
+                ng=0, ng_pass=None, device=0, recon="plm", protect=False):
     nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(n)
     c = ImhdConfig()
     lib().imhd_default_config(ctypes.byref(c))
@@ -33,6 +33,7 @@ def make_config(n, precision=32, riemann="roe", npass=0, sound_speed=1.0, cour=0
     c.ng = int(ng)
     c.ng_pass = int(ng if ng_pass is None else ng_pass)
     c.device = int(device)
+    c.protect = 1 if protect else 0
     return c
 
 

@@ -43,7 +43,7 @@ class Box:
     """A periodic box with nx*ny*nz interior cells, dx = 1/max(n)."""
 
     def __init__(self, n, precision=64, riemann="hlld", recon="plm", npass=1, sound_speed=1.0, cour=0.35,
-                 edot=1.0e-3, dt_turb=0.05, ng=0, ng_pass=None, device=0):
+                 edot=1.0e-3, dt_turb=0.05, ng=0, ng_pass=None, device=0, protect=False):
         nx, ny, nz = (n, n, n) if np.isscalar(n) else tuple(n)
         cfg = ImhdConfig()
         lib().imhd_default_config(ctypes.byref(cfg))
@@ -59,6 +59,7 @@ class Box:
         cfg.ng = int(ng)
         cfg.ng_pass = int(ng if ng_pass is None else ng_pass)
         cfg.device = int(device)
+        cfg.protect = 1 if protect else 0     # flux_protection of a Roe box (vanleer_mod.f90:81)
         self.cfg = cfg
         self.shape = (int(nz), int(ny), int(nx))
         self.npass = int(npass)

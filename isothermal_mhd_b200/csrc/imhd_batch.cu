@@ -179,6 +179,8 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
         if (c.recon < IMHD_PLM || c.recon > IMHD_PPM_PRIM) return bfail(IMHD_E_ARG, "recon must be IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM");
         if (c.npass < 0 || c.npass > imhd::kMaxPass) return bfail(IMHD_E_ARG, "npass must be in 0..8");
         if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return bfail(IMHD_E_ARG, "sound_speed and cour must be positive");
+        if (c.protect != 0 && c.protect != 1) return bfail(IMHD_E_ARG, "protect must be 0 or 1");
+        if (c.protect && c.riemann != IMHD_ROE) return bfail(IMHD_E_ARG, "protect needs IMHD_ROE");
     }
     int ndev = 0;
     BCK(cudaGetDeviceCount(&ndev));
@@ -194,7 +196,8 @@ int imhd_batch_create(const imhd_config* cfgs, int nbox, imhd_batch** out) {
     bool forcing = false;
     for (int i = 0; i < nbox; ++i) {
         const imhd_config& c = cfgs[i];
-        imhd::init_rec(x->rec[i], c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
+        imhd::init_rec(x->rec[i], c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb,
+                       c.protect);
         total += imhd::box_bytes(x->rec[i], x->esz, true);
         if ((size_t)x->rec[i].n > maxn) maxn = x->rec[i].n;
         forcing = forcing || c.edot > 0.0;
@@ -520,7 +523,7 @@ int imhd_batch_clock(imhd_batch* x, int box, double* t, long long* steps, double
     if (steps) *steps = s.steps_done;
     if (dt) *dt = s.dt;
     if (active) *active = s.active;
-    if (s.status & (IMHD_S_NAN | IMHD_S_ZERO_SPEED | IMHD_S_FORCE))
+    if (s.status & (IMHD_S_NAN | IMHD_S_ZERO_SPEED | IMHD_S_FORCE | IMHD_S_PROTECT))
         return bfail(IMHD_E_PHYSICS, "box stopped on a physics error (non-finite state, zero max speed or forcing)");
     return IMHD_OK;
 }

@@ -306,6 +306,9 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     if (c.npass < 0 || c.npass > imhd::kMaxPass) return fail(IMHD_E_ARG, "npass must be in 0..8");
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) return fail(IMHD_E_ARG, "sound_speed and cour must be positive");
     if (c.ng < 0 || c.ng_pass < 0) return fail(IMHD_E_ARG, "ghost widths must be >= 0");
+    if (c.protect != 0 && c.protect != 1) return fail(IMHD_E_ARG, "protect must be 0 or 1");
+    if (c.protect && c.riemann != IMHD_ROE)
+        return fail(IMHD_E_ARG, "protect needs IMHD_ROE (the reference computes protection fluxes for Roe only)");
     int ndev = 0;
     CK(cudaGetDeviceCount(&ndev));
     if (c.device < 0 || c.device >= ndev) return fail(IMHD_E_ARG, "no such CUDA device");
@@ -314,7 +317,8 @@ int imhd_create(const imhd_config* cfg, imhd_box** out) {
     imhd_box* x = new imhd_box();
     x->cfg = c;
     x->esz = c.precision == 64 ? 8 : 4;
-    imhd::init_rec(x->rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
+    imhd::init_rec(x->rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb,
+                   c.protect);
     imhd::BatchDev& b = x->b;
     b.precision = c.precision;
     size_t N = (size_t)x->rec.n;
@@ -451,6 +455,7 @@ int imhd_step(imhd_box* x, double dt, int drive_next, double* dt_next) {
     if (st & IMHD_S_NAN) return fail(IMHD_E_PHYSICS, "non-finite state or max speed: the step is not valid");
     if (st & IMHD_S_ZERO_SPEED) return fail(IMHD_E_PHYSICS, "zero max speed encountered");
     if (st & IMHD_S_FORCE) return fail(IMHD_E_PHYSICS, "bad value in turbulence driver energy normalisation");
+    if (st & IMHD_S_PROTECT) return fail(IMHD_E_PHYSICS, "more bad cells than the protection list holds");
     return IMHD_OK;
 }
 

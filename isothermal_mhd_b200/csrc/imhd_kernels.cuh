@@ -195,11 +195,31 @@ __device__ __forceinline__ void rotated(const CellQ<T>& a, T bn, T* u) {
     u[6] = a.q[R::BT2];
 }
 
+// Solver 4 (Roe with flux_protection, vanleer_mod.f90:81): the HLLE flux of
+// the same interface states into the protection buffer Fp, and the HLLE
+// wave speeds into smax, as the reference's extra compute_HLLE_fluxes_1d
+// call does (:540, 703, 880, 2962).  Nothing for the other solvers.
+template <class T, int SOLVER>
+__device__ __forceinline__ void protection_flux(const T* uL, const T* uR, T cs, T asqr, T& smax, void* Fp, int D, int n,
+                                                int c) {
+    if constexpr (SOLVER == 4) {
+        T Fh[7];
+        riemann_flux<3>(uL, uR, cs, asqr, Fh, smax);
+        T* Fd = (T*)Fp + (size_t)(6 * D) * n;
+        Fd[c] = Fh[0];
+        Fd[(size_t)n + c] = Fh[1];
+        Fd[2 * (size_t)n + c] = Fh[2];
+        Fd[3 * (size_t)n + c] = Fh[3];
+        Fd[4 * (size_t)n + c] = Fh[5];
+        Fd[5 * (size_t)n + c] = Fh[6];
+    }
+}
+
 // FP32 occupancy, measured at 512^3: five blocks per SM for the Roe solver
 // (96 registers; fewer registers spill more than the extra warps return), six
 // for HLLD and HLLE (80 registers, 3.9 -> 3.7 ms).
 template <class T, int SCHEME, bool ONE>
-__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? (scheme_solver(SCHEME) == 1 ? 5 : 6) : 1)
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? (scheme_solver(SCHEME) % 3 == 1 ? 5 : 6) : 1)
 k_pred_flux(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     int local;
@@ -241,6 +261,7 @@ k_pred_flux(BatchArgs ba) {
                 Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
                 Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
             }
+            protection_flux<T, SOLVER>(uL, uR, cs, asqr, sref, rp.Fp, 0, n, c);
             // y face
             rotated<T, 1>(cur, cur.q[8], uL);
             rotated<T, 1>(yn, cur.q[8], uR);
@@ -250,6 +271,7 @@ k_pred_flux(BatchArgs ba) {
                 Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
                 Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
             }
+            protection_flux<T, SOLVER>(uL, uR, cs, asqr, sref, rp.Fp, 1, n, c);
             // z face
             rotated<T, 2>(cur, cur.q[9], uL);
             rotated<T, 2>(zn, cur.q[9], uR);
@@ -259,6 +281,7 @@ k_pred_flux(BatchArgs ba) {
                 Fd[c] = Fo[0]; Fd[(size_t)n + c] = Fo[1]; Fd[2 * (size_t)n + c] = Fo[2];
                 Fd[3 * (size_t)n + c] = Fo[3]; Fd[4 * (size_t)n + c] = Fo[5]; Fd[5 * (size_t)n + c] = Fo[6];
             }
+            protection_flux<T, SOLVER>(uL, uR, cs, asqr, sref, rp.Fp, 2, n, c);
             cur = zn;
         }
     }
@@ -356,8 +379,10 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march
                 plm_right_state(wc, dB, bnA, qR);
                 const int kf = (D == 1) ? o : a;
                 T sdrop = T(0);
-                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop);
+                T& sref = (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop;
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, sref);
                 store_flux(F, D, dm.n, base + a * stride, Fo);
+                protection_flux<T, SOLVER>(qL, qR, cs, asqr, sref, rp.Fp, D, dm.n, base + a * stride);
 #pragma unroll
                 for (int m = 0; m < 6; ++m) { wb_[m] = wc[m]; wc[m] = wd[m]; dA[m] = dB[m]; }
                 bnA = bnB; bnB = bnC;
@@ -388,8 +413,10 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corr_flux_march
                 ppm_state(l1, bn0, qR);
                 const int kf = (D == 1) ? o : a;
                 T sdrop = T(0);
-                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop);
+                T& sref = (kf >= rp.zlo && kf < rp.zhi) ? smax : sdrop;
+                riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, sref);
                 store_flux(F, D, dm.n, base + a * stride, Fo);
+                protection_flux<T, SOLVER>(qL, qR, cs, asqr, sref, rp.Fp, D, dm.n, base + a * stride);
 #pragma unroll
                 for (int m = 0; m < 6; ++m) {
                     w0[m] = w1[m]; w1[m] = w2[m]; w2[m] = w3[m];
@@ -484,8 +511,10 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
             ppm_state(l1, bn, qR);
         }
         T sdrop = T(0);
-        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
+        T& sref = (k >= rp.zlo && k < rp.zhi) ? smax : sdrop;
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, sref);
         store_flux(F, 0, dm.n, row + i, Fo);
+        protection_flux<T, SOLVER>(qL, qR, cs, asqr, sref, rp.Fp, 0, dm.n, row + i);
     }
     block_atomic_max<TX>(smax_slots, (double)smax);
 }
@@ -573,8 +602,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(
             ppm_state(l1, bn, qR);
         }
         T sdrop = T(0);
-        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, (k >= rp.zlo && k < rp.zhi) ? smax : sdrop);
+        T& sref = (k >= rp.zlo && k < rp.zhi) ? smax : sdrop;
+        riemann_flux<SOLVER>(qL, qR, cs, asqr, Fo, sref);
         store_flux(F, 0, dm.n, row + i, Fo);
+        protection_flux<T, SOLVER>(qL, qR, cs, asqr, sref, rp.Fp, 0, dm.n, row + i);
     }
     block_atomic_max_any(smax_slots, (double)smax);
 }
@@ -634,15 +665,18 @@ __device__ __forceinline__ CellEV<T> cell_ev(const T* __restrict__ S, int n, int
 // velocities of plane k+1 computed at one step are those of plane k at the
 // next, and so are the z-face EMFs read at k+1, so each is loaded and
 // computed once per column instead of once per neighbour.
-template <class T, bool ONE>
+// PROT: the corner EMFs of the protection fluxes (Fp -> Ep) of the boxes
+// that compute them, the second compute_cell_corner_emf_3d call of
+// vanleer_mod.f90:336, 396 (the cell-centre EMFs are the same).
+template <class T, bool ONE, bool PROT = false>
 __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(BatchArgs ba, int half_step_state) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
-    if (!rp.active) return;
+    if (!rp.active || (PROT && !rp.protect)) return;
     const Dims dm = dims_of(rp);
     const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
-    const T* __restrict__ F = (const T*)rp.F;
-    T* __restrict__ E = (T*)rp.E;
+    const T* __restrict__ F = (const T*)(PROT ? rp.Fp : rp.F);
+    T* __restrict__ E = (T*)(PROT ? rp.Ep : rp.E);
     int i, j, k0, k1;
     decode_cellz<ONE>(local, dm, rp.tws, rp.segzs, i, j, k0, k1);
     if (i >= dm.nx || j >= dm.ny) return;
@@ -764,6 +798,18 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
     return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
 }
 
+// Flux protection (flux_protection, vanleer_mod.f90:81, 2086-2202): a cell
+// whose updated density fell below MIN_DENS is flagged and listed for the
+// protection kernels of this update stage (0 predictor, 1 final).  A list
+// that overflows sets IMHD_S_PROTECT.
+constexpr unsigned kStatusProtect = 32u;   // IMHD_S_PROTECT
+__device__ __forceinline__ void prot_mark_bad(const BoxRec& r, int stage, int c) {
+    r.bad[c] = 1;
+    const unsigned slot = atomicAdd(&r.sc->nbad[stage], 1u);
+    if (slot < (unsigned)r.badcap) r.badlist[(size_t)stage * r.badcap + slot] = c;
+    else atomicOr(&r.sc->status, kStatusProtect);
+}
+
 // A table's box goes to the bulk-copy fed update when its rows are whole
 // 128-cell tiles (or 64-cell tiles with an even row count: a block then takes
 // two rows) and the bases its copies read from are 16-byte aligned (both
@@ -844,7 +890,8 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
             const bool inz = !ZR || (k >= rp.zlo && k < rp.zhi);
             if (out[0] < T(kMIN_DENS)) {
                 out[0] = T(kMIN_DENS);
-                if (inz) atomicAdd(floor_hits, 1ull);
+                if (rp.protect) prot_mark_bad(rp, final_stage, c);   // updated again by k_prot_hydro
+                else if (inz) atomicAdd(floor_hits, 1ull);
             }
             const T Ex0 = Ex[c], Ey0 = Ey[c], Ez0 = E[2 * (size_t)n + c];
             const T Ex_ym = Ex[cym], Ey_xm = Ey[cxm];
@@ -1062,7 +1109,8 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
             const bool inz = !ZR || (k >= rp.zlo && k < rp.zhi);
             if (out[0] < T(kMIN_DENS)) {
                 out[0] = T(kMIN_DENS);
-                if (inz) atomicAdd(&sc->floor_hits, 1ull);
+                if (rp.protect) prot_mark_bad(rp, final_stage, c);   // updated again by k_prot_hydro
+                else if (inz) atomicAdd(&sc->floor_hits, 1ull);
             }
             const T Ex0 = at(19), Ey0 = at(20), Ez0 = at(21);
             const T Ex_ym = at(27), Ey_xm = xm(20, 5);
@@ -1104,6 +1152,216 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
         mbar_wait(&bars[last & 1], (unsigned)((last >> 1) & 1));
     }
     if (do_cfl) block_atomic_max<kTmaTile>(cmax_slots, cmax);
+}
+
+// ============================================================ flux protection
+// The protected update of update_hydro_state_3d (vanleer_mod.f90:2086-2202)
+// after an update stage that listed bad cells (prot_mark_bad).  The
+// reference, for every bad cell, copies the protection (HLLE) fluxes of its
+// six faces into the flux array and the protection corner EMFs of the four
+// corners (i,j,k), (i-1,j,k), (i,j-1,k), (i,j,k-1) of each component into
+// the corner array (:2147-2171), then updates the bad cells and their six
+// neighbours again from the state before the update (:2179-2201); the CT
+// update that follows uses the replaced corners.  So a face takes the
+// protection flux when a cell on either side is bad, and corner (i,j,k) takes
+// the protection EMF when one of the cells (i,j,k), (i+1,j,k), (i,j+1,k),
+// (i,j,k+1) is bad.  kProtBlocks blocks per box walk the stage's list; a cell
+// reached from several bad cells is written by the smallest of them (hydro)
+// or rewritten with the same value (faces, cell centres).
+constexpr int kProtBlocks = 32;
+
+template <bool ONE>
+__device__ __forceinline__ BoxRec prot_box(const BatchArgs& ba, int& local) {
+    const int b = ONE ? 0 : (int)blockIdx.x / kProtBlocks;
+    local = ONE ? (int)blockIdx.x : (int)blockIdx.x % kProtBlocks;
+    return box_at(ba, b);
+}
+__device__ __forceinline__ int cell_at(const Dims& dm, int i, int j, int k) {
+    return wrap_any(i, dm.nx) + dm.nx * (wrap_any(j, dm.ny) + dm.ny * wrap_any(k, dm.nz));
+}
+__device__ __forceinline__ void cell_ijk(const Dims& dm, int c, int& i, int& j, int& k) {
+    const int plane = dm.nx * dm.ny;
+    i = c % dm.nx;
+    j = (c % plane) / dm.nx;
+    k = c / plane;
+}
+// corner of component m (0 Ex, 1 Ey, 2 Ez) at cell (i,j,k) takes the protection EMF
+__device__ __forceinline__ bool prot_corner(const unsigned char* __restrict__ bad, const Dims& dm, int i, int j, int k) {
+    return bad[cell_at(dm, i, j, k)] | bad[cell_at(dm, i + 1, j, k)] | bad[cell_at(dm, i, j + 1, k)] |
+           bad[cell_at(dm, i, j, k + 1)];
+}
+
+// Hydro variables of the bad cells and their neighbours, again from the
+// state before the update with the protection fluxes on the faces of bad
+// cells, then final_check_unphysical (:3243-3262) for them.
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_prot_hydro(BatchArgs ba, double dt_scale, int stage) {
+    int local;
+    const BoxRec rp = prot_box<ONE>(ba, local);
+    if (!rp.active || !rp.protect) return;
+    Scalars* sc = rp.sc;
+    const unsigned nb = min(sc->nbad[stage], (unsigned)rp.badcap);
+    if (nb == 0) return;
+    const Dims dm = dims_of(rp);
+    const int n = dm.n;
+    const int* __restrict__ list = rp.badlist + (size_t)stage * rp.badcap;
+    const unsigned char* __restrict__ bad = rp.bad;
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ Sout = (T*)rp.S[1];
+    const T* __restrict__ F = (const T*)rp.F;
+    const T* __restrict__ Fp = (const T*)rp.Fp;
+    const T dtdx = (T)(dt_scale * sc->dt / rp.dx);
+    for (long w = (long)local * blockDim.x + threadIdx.x; w < 7L * nb; w += (long)kProtBlocks * blockDim.x) {
+        const int b = list[w / 7];
+        const int slot = (int)(w % 7);
+        int i, j, k;
+        cell_ijk(dm, b, i, j, k);
+        if (slot == 1) --i; else if (slot == 2) ++i;
+        else if (slot == 3) --j; else if (slot == 4) ++j;
+        else if (slot == 5) --k; else if (slot == 6) ++k;
+        const int c = cell_at(dm, i, j, k);
+        const int cxm = cell_at(dm, i - 1, j, k), cxp = cell_at(dm, i + 1, j, k);
+        const int cym = cell_at(dm, i, j - 1, k), cyp = cell_at(dm, i, j + 1, k);
+        const int czm = cell_at(dm, i, j, k - 1), czp = cell_at(dm, i, j, k + 1);
+        const bool b0 = bad[c], bxm = bad[cxm], bxp = bad[cxp], bym = bad[cym], byp = bad[cyp];
+        const bool bzm = bad[czm], bzp = bad[czp];
+        // the smallest bad cell next to c (or c itself) writes it
+        int owner = 0x7fffffff;
+        if (b0) owner = c;
+        if (bxm && cxm < owner) owner = cxm;
+        if (bxp && cxp < owner) owner = cxp;
+        if (bym && cym < owner) owner = cym;
+        if (byp && cyp < owner) owner = cyp;
+        if (bzm && czm < owner) owner = czm;
+        if (bzp && czp < owner) owner = czp;
+        if (owner != b) continue;
+        const bool px = b0 || bxp, pxm = bxm || b0, py = b0 || byp, pym = bym || b0, pz = b0 || bzp, pzm = bzm || b0;
+        T out[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int fx = (v == 0) ? 0 : 1 + (v - 1 + 3) % 3;
+            const int fy = (v == 0) ? 0 : 1 + (v - 1 - 1 + 3) % 3;
+            const int fz = (v == 0) ? 0 : 1 + (v - 1 - 2 + 3) % 3;
+            const T Fxc = (px ? Fp : F)[(size_t)fx * n + c], Fxm = (pxm ? Fp : F)[(size_t)fx * n + cxm];
+            const T Fyc = (py ? Fp : F)[(size_t)(6 + fy) * n + c], Fym = (pym ? Fp : F)[(size_t)(6 + fy) * n + cym];
+            const T Fzc = (pz ? Fp : F)[(size_t)(12 + fz) * n + c], Fzm = (pzm ? Fp : F)[(size_t)(12 + fz) * n + czm];
+            out[v] = fld(S0, v, n)[c] - dtdx * ((Fxc - Fxm) + (Fyc - Fym) + (Fzc - Fzm));
+        }
+        const bool inz = k >= rp.zlo && k < rp.zhi;
+        if (out[0] < T(kMIN_DENS)) {
+            out[0] = T(kMIN_DENS);
+            if (inz) atomicAdd(&sc->floor_hits, 1ull);
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
+        if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3])))
+            atomicOr(&sc->status, 2u);
+    }
+}
+
+// Face fields around the bad cells with the protection corner EMFs where
+// they replace the corners (update_CT_3d, :2211-2245).
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_prot_faces(BatchArgs ba, double dt_scale, int stage) {
+    int local;
+    const BoxRec rp = prot_box<ONE>(ba, local);
+    if (!rp.active || !rp.protect) return;
+    Scalars* sc = rp.sc;
+    const unsigned nb = min(sc->nbad[stage], (unsigned)rp.badcap);
+    if (nb == 0) return;
+    const Dims dm = dims_of(rp);
+    const int n = dm.n;
+    const int* __restrict__ list = rp.badlist + (size_t)stage * rp.badcap;
+    const unsigned char* __restrict__ bad = rp.bad;
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ Sout = (T*)rp.S[1];
+    const T* __restrict__ E = (const T*)rp.E;
+    const T* __restrict__ Ep = (const T*)rp.Ep;
+    const T dtdx = (T)(dt_scale * sc->dt / rp.dx);
+    // corner EMF of component m at cell (i,j,k): the protection value where replaced
+    auto corner = [&](int m, int i, int j, int k) -> T {
+        const int q = cell_at(dm, i, j, k);
+        return (prot_corner(bad, dm, i, j, k) ? Ep : E)[(size_t)m * n + q];
+    };
+    for (long w = (long)local * blockDim.x + threadIdx.x; w < 27L * nb; w += (long)kProtBlocks * blockDim.x) {
+        int i, j, k;
+        cell_ijk(dm, list[w / 27], i, j, k);
+        const int o = (int)(w % 27);
+        i += o % 3 - 1;
+        j += (o / 3) % 3 - 1;
+        k += o / 9 - 1;
+        const int c = cell_at(dm, i, j, k);
+        const T Ex0 = corner(0, i, j, k), Ey0 = corner(1, i, j, k), Ez0 = corner(2, i, j, k);
+        const T bx = fld(S0, 7, n)[c] - dtdx * ((Ez0 - corner(2, i, j - 1, k)) - (Ey0 - corner(1, i, j, k - 1)));
+        const T by = fld(S0, 8, n)[c] - dtdx * ((Ex0 - corner(0, i, j, k - 1)) - (Ez0 - corner(2, i - 1, j, k)));
+        const T bz = fld(S0, 9, n)[c] - dtdx * ((Ey0 - corner(1, i - 1, j, k)) - (Ex0 - corner(0, i, j - 1, k)));
+        fld(Sout, 7, n)[c] = bx;
+        fld(Sout, 8, n)[c] = by;
+        fld(Sout, 9, n)[c] = bz;
+        const int kk = wrap_any(k, dm.nz);
+        if (kk >= rp.zlo && kk < rp.zhi && !(isfinite(bx) && isfinite(by) && isfinite(bz))) atomicOr(&sc->status, 2u);
+    }
+}
+
+// Cell-centred field of the cells next to those faces (update_CT_3d, :2248-2259).
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kBX) k_prot_centres(BatchArgs ba, int stage) {
+    int local;
+    const BoxRec rp = prot_box<ONE>(ba, local);
+    if (!rp.active || !rp.protect) return;
+    Scalars* sc = rp.sc;
+    const unsigned nb = min(sc->nbad[stage], (unsigned)rp.badcap);
+    if (nb == 0) return;
+    const Dims dm = dims_of(rp);
+    const int n = dm.n;
+    const int* __restrict__ list = rp.badlist + (size_t)stage * rp.badcap;
+    T* __restrict__ Sout = (T*)rp.S[1];
+    for (long w = (long)local * blockDim.x + threadIdx.x; w < 64L * nb; w += (long)kProtBlocks * blockDim.x) {
+        int i, j, k;
+        cell_ijk(dm, list[w / 64], i, j, k);
+        const int o = (int)(w % 64);
+        i += o % 4 - 1;
+        j += (o / 4) % 4 - 1;
+        k += o / 16 - 1;
+        const int c = cell_at(dm, i, j, k);
+        fld(Sout, 4, n)[c] = T(0.5) * (fld(Sout, 7, n)[c] + fld(Sout, 7, n)[cell_at(dm, i - 1, j, k)]);
+        fld(Sout, 5, n)[c] = T(0.5) * (fld(Sout, 8, n)[c] + fld(Sout, 8, n)[cell_at(dm, i, j - 1, k)]);
+        fld(Sout, 6, n)[c] = T(0.5) * (fld(Sout, 9, n)[c] + fld(Sout, 9, n)[cell_at(dm, i, j, k - 1)]);
+    }
+}
+
+// The final stage's CFL maximum of the corrected state, into cfl_slots, when
+// the stage had bad cells (k_finalize then takes it instead of the update's).
+template <class T, bool ONE>
+__global__ void __launch_bounds__(kRedThreads) k_prot_cfl(BatchArgs ba) {
+    int local;
+    const BoxRec rp = resolve<ONE>(ba, kKindRed, local);
+    if (!rp.active || !rp.protect) return;
+    Scalars* sc = rp.sc;
+    if (sc->nbad[1] == 0 || sc->drive) return;
+    const T* __restrict__ S = (const T*)rp.S[1];
+    const T asqr = (T)(rp.cs * rp.cs);
+    const int n = rp.n, plane = rp.nx * rp.ny;
+    double cm = 0.0;
+    for (int c = local * blockDim.x + threadIdx.x; c < n; c += rp.nred * blockDim.x) {
+        const int kc = c / plane;
+        if (kc < rp.zlo || kc >= rp.zhi) continue;
+        cm = nmax(cm, (double)cell_max_speed(fld(S, 0, n)[c], fld(S, 1, n)[c], fld(S, 2, n)[c], fld(S, 3, n)[c],
+                                             fld(S, 4, n)[c], fld(S, 5, n)[c], fld(S, 6, n)[c], asqr));
+    }
+    block_atomic_max<kRedThreads>(sc->cfl_slots, cm);
+}
+
+// Clear the bad flags of a stage's list (the counts are reset by k_finalize).
+template <bool ONE>
+__global__ void __launch_bounds__(kBX) k_prot_clear(BatchArgs ba, int stage) {
+    int local;
+    const BoxRec rp = prot_box<ONE>(ba, local);
+    if (!rp.active || !rp.protect) return;
+    const unsigned nb = min(rp.sc->nbad[stage], (unsigned)rp.badcap);
+    const int* __restrict__ list = rp.badlist + (size_t)stage * rp.badcap;
+    for (long w = (long)local * blockDim.x + threadIdx.x; w < (long)nb; w += (long)kProtBlocks * blockDim.x)
+        rp.bad[list[w]] = 0;
 }
 
 // ============================================================ passive scalars
@@ -1487,14 +1745,19 @@ static __global__ void k_finalize(BatchArgs ba, int device_driven) {
     const double cour = rp.cour, dx = rp.dx;
     const int drive = sc->drive;
     double cell = 0.0, smax = 0.0, dvm = 0.0;
+    // after a protected final update with bad cells the CFL maximum of the
+    // corrected state is in cfl_slots (k_prot_cfl)
+    const bool protected_cfl = rp.protect && sc->nbad[1] > 0 && !drive;
     for (int s = 0; s < kSlots; ++s) {
-        cell = nmax(cell, __longlong_as_double((long long)sc->cmax_slots[s]));
+        cell = nmax(cell, __longlong_as_double((long long)(protected_cfl ? sc->cfl_slots[s] : sc->cmax_slots[s])));
         smax = nmax(smax, __longlong_as_double((long long)sc->smax_slots[s]));
         dvm = nmax(dvm, __longlong_as_double((long long)sc->dvmax_slots[s]));
         sc->cmax_slots[s] = 0ull;
         sc->smax_slots[s] = 0ull;
         sc->dvmax_slots[s] = 0ull;
+        if (rp.protect) sc->cfl_slots[s] = 0ull;
     }
+    sc->nbad[0] = sc->nbad[1] = 0u;
     double cmax = vmax(cell, smax + dvm);
     if (!(cmax == cmax) || cmax > 1.0e300) sc->status |= 2u;
     if (cmax < kZERO) sc->status |= 4u;
@@ -1514,7 +1777,7 @@ static __global__ void k_finalize(BatchArgs ba, int device_driven) {
         // driver.f90:86-87 and :475 for this box
         sc->t = sc->t + sc->dt;
         sc->steps_done += 1;
-        if (sc->steps_done >= sc->steps_target || !(sc->t < sc->t_end) || (sc->status & 6u)) {
+        if (sc->steps_done >= sc->steps_target || !(sc->t < sc->t_end) || (sc->status & (6u | kStatusProtect))) {
             sc->active = 0;
             if (!ba.use_one) ba.boxes[b].active = 0;
         } else {

@@ -181,6 +181,26 @@ static void launch_fluxes_corr_march(BatchDev& b) {
     b.launches += 1;
 }
 
+// The protected update of flux_protection after update stage `stage`
+// (vanleer_mod.f90:2086-2202): hydro variables of the bad cells and their
+// neighbours, face fields, cell-centred field, the CFL maximum after the
+// final stage, then the bad flags cleared.  Every kernel returns at once for
+// a box whose stage listed no bad cell.
+template <class T, bool ONE>
+static void launch_protection(BatchDev& b, double dt_scale, int stage) {
+    const unsigned g = ONE ? (unsigned)kProtBlocks : (unsigned)(kProtBlocks * b.a.nbox);
+    k_prot_hydro<T, ONE><<<g, kBX, 0, b.st>>>(b.a, dt_scale, stage);
+    k_prot_faces<T, ONE><<<g, kBX, 0, b.st>>>(b.a, dt_scale, stage);
+    k_prot_centres<T, ONE><<<g, kBX, 0, b.st>>>(b.a, stage);
+    b.launches += 3;
+    if (stage == 1) {
+        k_prot_cfl<T, ONE><<<b.totals[kKindRed], kRedThreads, 0, b.st>>>(b.a);
+        b.launches += 1;
+    }
+    k_prot_clear<ONE><<<g, kBX, 0, b.st>>>(b.a, stage);
+    b.launches += 1;
+}
+
 template <class T, bool ONE>
 static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     const dim3 gc = grid_of<ONE>(b, kKindCell);
@@ -203,8 +223,13 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStPredEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
     b.launches += 1;
+    if (b.any_protect) {
+        k_corner_emf<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 0);
+        b.launches += 1;
+    }
     mark(b, kStPredUpdate);
     launch_update<T, ONE>(b, 0.5, 0);   // counts its own launches
+    if (b.any_protect) launch_protection<T, ONE>(b, 0.5, 0);
     // corrector: characteristic PLM fluxes of the half-step state, EMFs,
     // full-dt update of the step-start state
     mark(b, kStCorrFluxX);
@@ -216,8 +241,13 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStCorrEmf);
     k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
     b.launches += 1;
+    if (b.any_protect) {
+        k_corner_emf<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 1);
+        b.launches += 1;
+    }
     mark(b, kStFinalUpdate);
     launch_update<T, ONE>(b, 1.0, 1);
+    if (b.any_protect) launch_protection<T, ONE>(b, 1.0, 1);
     if (b.drive_mode) {
         mark(b, kStForceKick);
         k_force_kick<T, ONE><<<gc, kBX, 0, b.st>>>(b.a);

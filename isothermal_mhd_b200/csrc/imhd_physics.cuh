@@ -380,7 +380,7 @@ __device__ __forceinline__ void flux_hlld(const T* uL, const T* uR, T asqr, T* F
 
 template <int SOLVER, class T>
 __device__ __forceinline__ void riemann(const T* uL, const T* uR, T cs, T asqr, T* Fo, T& smax) {
-    if (SOLVER == 1) flux_roe(uL, uR, cs, asqr, Fo, smax);
+    if (SOLVER == 1 || SOLVER == 4) flux_roe(uL, uR, cs, asqr, Fo, smax);   // 4: Roe with protection fluxes
     else if (SOLVER == 2) flux_hlld(uL, uR, asqr, Fo, smax);
     else flux_hlle(uL, uR, asqr, Fo, smax);
 }

@@ -401,7 +401,7 @@ namespace imhd {
 template <int SOLVER, class T>
 __device__ __forceinline__ void riemann_flux(const T* uL, const T* uR, T cs, T asqr, T* Fo, T& smax) {
     if constexpr (std::is_same<T, float>::value) {
-        if (SOLVER == 1) flux_roe_fast(uL, uR, cs, asqr, Fo, smax);
+        if (SOLVER == 1 || SOLVER == 4) flux_roe_fast(uL, uR, cs, asqr, Fo, smax);
         else if (SOLVER == 2) flux_hlld_fast(uL, uR, asqr, Fo, smax);
         else flux_hlle_fast(uL, uR, asqr, Fo, smax);
     } else {

@@ -122,6 +122,8 @@ bool valid_box(const imhd_config& c, std::string& why) {
     if ((double)c.nx * c.ny * c.nz >= 2147483647.0) { why = "box too large"; return false; }
     if (c.riemann < 1 || c.riemann > 3) { why = "riemann must be IMHD_ROE, IMHD_HLLD or IMHD_HLLE"; return false; }
     if (c.recon < IMHD_PLM || c.recon > IMHD_PPM_PRIM) { why = "recon must be IMHD_PLM, IMHD_PPM, IMHD_PLM_PRIM or IMHD_PPM_PRIM"; return false; }
+    if (c.protect != 0 && c.protect != 1) { why = "protect must be 0 or 1"; return false; }
+    if (c.protect && c.riemann != IMHD_ROE) { why = "protect needs IMHD_ROE"; return false; }
     if (c.npass < 0 || c.npass > imhd::kMaxPass) { why = "npass must be in 0..8"; return false; }
     if (!(c.sound_speed > 0.0) || !(c.cour > 0.0)) { why = "sound_speed and cour must be positive"; return false; }
     if (c.ng < 0 || c.ng_pass < 0) { why = "ghost widths must be >= 0"; return false; }
@@ -197,7 +199,8 @@ struct Worker {
     bool build(Resident& r) {
         const Request& q = r.req;
         const imhd_config& c = q.cfg;
-        imhd::init_rec(r.rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb);
+        imhd::init_rec(r.rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb,
+                       c.protect);
         r.bytes = imhd::box_bytes(r.rec, s->esz, q.forcing != 0);
         cudaError_t e = cudaMallocAsync(&r.mem, r.bytes, st);
         if (e != cudaSuccess) {
@@ -336,7 +339,7 @@ struct Worker {
                 const Request& h = s->queue.front();
                 imhd::BoxRec probe;
                 imhd::init_rec(probe, h.cfg.nx, h.cfg.ny, h.cfg.nz, h.cfg.npass, h.cfg.riemann, h.cfg.recon, h.cfg.sound_speed,
-                               h.cfg.cour, h.cfg.edot, h.cfg.dt_turb);
+                               h.cfg.cour, h.cfg.edot, h.cfg.dt_turb, h.cfg.protect);
                 size_t need = imhd::box_bytes(probe, s->esz, h.forcing != 0);
                 long long cells = (long long)h.cfg.nx * h.cfg.ny * h.cfg.nz;
                 bool over_budget = (double)(s->used_bytes + need) > s->cfg.hbm_budget_bytes;
@@ -408,7 +411,7 @@ struct Worker {
             const double* c = clocks_host + (size_t)i * kClockWords;
             r.cur = (int)c[3];
             const unsigned status = (unsigned)c[4];
-            const bool bad = (status & (IMHD_S_NAN | IMHD_S_ZERO_SPEED | IMHD_S_FORCE)) != 0;
+            const bool bad = (status & (IMHD_S_NAN | IMHD_S_ZERO_SPEED | IMHD_S_FORCE | IMHD_S_PROTECT)) != 0;
             if (c[2] != 0.0 && !bad) {
                 keep.push_back(std::move(r));
                 continue;

@@ -35,7 +35,7 @@ inline long blocks_of(const BoxRec& r, int kind, size_t esz) {
                    : 0;
     int scheme = 1 + (kind - kKindSolver0) / 5;
     int sub = (kind - kKindSolver0) % 5;
-    if (scheme_of(r.riemann, r.recon) != scheme) return 0;
+    if (scheme_of(box_solver(r), r.recon) != scheme) return 0;
     bool row = row_capable(r.nx, esz);
     switch (sub) {
         case kSubCell: return nbx * nby * ceil_div(r.nz, kSegZ);   // z columns of the predictor fluxes
@@ -82,9 +82,11 @@ inline bool build_prefix(const std::vector<BoxRec>& recs, size_t esz, std::vecto
     bd.any_pass = false;
     bd.npass_max = 0;
     bd.any_zrange = false;
+    bd.any_protect = false;
     for (const BoxRec& r : recs) {
+        if (r.protect) bd.any_protect = true;
         if (r.riemann >= 1 && r.riemann <= 3 && r.recon >= 0 && r.recon < kRecons)
-            bd.has_scheme[scheme_of(r.riemann, r.recon)] = true;
+            bd.has_scheme[scheme_of(box_solver(r), r.recon)] = true;
         if (r.npass > 0) bd.any_pass = true;
         if (r.npass > bd.npass_max) bd.npass_max = r.npass;
         if (r.zlo != 0 || r.zhi != r.nz) bd.any_zrange = true;
@@ -155,13 +157,13 @@ inline void host_ghost_fill(int nx, int ny, int nz, double* h, int ng) {
 
 // Fill the geometry fields of a box record from its configuration.
 inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, int recon, double cs, double cour,
-                     double edot,
-                     double dt_turb) {
+                     double edot, double dt_turb, int protect = 0) {
     std::memset(&r, 0, sizeof(r));
     r.nx = nx; r.ny = ny; r.nz = nz; r.n = nx * ny * nz;
     r.npass = npass;
     r.riemann = riemann;
     r.recon = recon;
+    r.protect = (riemann == 1 && protect) ? 1 : 0;   // protection fluxes exist for the Roe solver only
     r.zlo = 0;
     r.zhi = nz;
     // widest x tile that the row length divides (whole 128-byte segments per
@@ -189,11 +191,15 @@ inline void init_rec(BoxRec& r, int nx, int ny, int nz, int npass, int riemann, 
 
 // Device bytes of one box's buffers (state x2, fluxes, EMFs, half-step
 // scalars, boundary planes, partial sums, scalars), each 256-byte aligned.
+// Capacity of a stage's bad-cell list under flux protection.
+inline int prot_list_cap(int n) { return n < (1 << 20) ? n : (1 << 20); }
 inline size_t box_bytes(const BoxRec& r, size_t esz, bool with_force) {
     size_t n = (size_t)r.n, nf = 10 + (size_t)r.npass;
     size_t b = 2 * align256(nf * n * esz) + align256(18 * n * esz) + align256(3 * n * esz);
     if (r.npass) b += align256((size_t)r.npass * n * esz) + align256(6 * (size_t)r.plane_stride * esz);
     if (with_force) b += align256(3 * n * esz);
+    if (r.protect)
+        b += align256(18 * n * esz) + align256(3 * n * esz) + align256(n) + align256(2 * (size_t)prot_list_cap(r.n) * 4);
     b += align256((size_t)r.nred * 6 * 8) + align256(sizeof(Scalars));
     return b;
 }
@@ -212,6 +218,15 @@ inline void carve_box(BoxRec& r, unsigned char* base, size_t esz, bool with_forc
         r.SH = nullptr; r.mbnd = nullptr;
     }
     if (with_force) { r.delv = p; p += align256(3 * n * esz); } else r.delv = nullptr;
+    if (r.protect) {   // the bad flags must start at zero: the whole pool is cleared after carving
+        r.Fp = p; p += align256(18 * n * esz);
+        r.Ep = p; p += align256(3 * n * esz);
+        r.bad = p; p += align256(n);
+        r.badcap = prot_list_cap(r.n);
+        r.badlist = (int*)p; p += align256(2 * (size_t)r.badcap * 4);
+    } else {
+        r.Fp = r.Ep = nullptr; r.bad = nullptr; r.badlist = nullptr; r.badcap = 0;
+    }
     r.partials = (double*)p; p += align256((size_t)r.nred * 6 * 8);
     r.sc = (Scalars*)p;
 }

@@ -32,20 +32,22 @@ enum Kind {
     kKindCell = 0,     // (x, y) tiles of kBX threads per z plane, one cell per thread
     kKindRed = 1,      // min(kRedBlocksMax, ceil(n/kRedThreads)) blocks, grid-stride reductions
     kKindSolver0 = 2,  // + 5*(scheme-1) + {z column (predictor), x-row, x-tile, march-y, march-z}, 0 blocks if the box uses another scheme
-    kKindCellZ = 62,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
-    kKindUpdTma = 63,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
-    kKindUpdTma64 = 64,// pairs of 64-cell row segments per z segment of it (rows of 64(2k+1) cells, even ny)
-    kKinds = 65
+    kKindCellZ = 82,   // (x, y) tiles per z segment, a z column of kSegZ cells per thread
+    kKindUpdTma = 83,  // 128-cell row segments per z segment of the bulk-copy fed update (rows of 128k cells)
+    kKindUpdTma64 = 84,// pairs of 64-cell row segments per z segment of it (rows of 64(2k+1) cells, even ny)
+    kKinds = 85
 };
-// A scheme is a Riemann solver (1 Roe, 2 HLLD, 3 HLLE) with a reconstruction
-// (0 PLM and 1 PPM of the characteristic variables, 2 PLM and 3 PPM of the
-// primitive variables): scheme = solver + 3 * recon, 1..kSchemes.
+// A scheme is a flux solver (1 Roe, 2 HLLD, 3 HLLE, 4 Roe with the HLLE
+// protection fluxes beside it) with a reconstruction (0 PLM and 1 PPM of the
+// characteristic variables, 2 PLM and 3 PPM of the primitive variables):
+// scheme = solver + 4 * recon, 1..kSchemes.
+constexpr int kSolvers = 4;
 constexpr int kRecons = 4;
-constexpr int kSchemes = 3 * kRecons;
+constexpr int kSchemes = kSolvers * kRecons;
 static_assert(kKindSolver0 + 5 * kSchemes == kKindCellZ, "block-decomposition kinds overlap");
-__host__ __device__ constexpr int scheme_of(int solver, int recon) { return solver + 3 * recon; }
-__host__ __device__ constexpr int scheme_solver(int scheme) { return 1 + (scheme - 1) % 3; }
-__host__ __device__ constexpr int scheme_recon(int scheme) { return (scheme - 1) / 3; }
+__host__ __device__ constexpr int scheme_of(int solver, int recon) { return solver + kSolvers * recon; }
+__host__ __device__ constexpr int scheme_solver(int scheme) { return 1 + (scheme - 1) % kSolvers; }
+__host__ __device__ constexpr int scheme_recon(int scheme) { return (scheme - 1) / kSolvers; }
 __host__ __device__ constexpr int scheme_kind(int scheme, int sub) { return kKindSolver0 + 5 * (scheme - 1) + sub; }
 enum SolverSub { kSubCell = 0, kSubXRow = 1, kSubXTile = 2, kSubMarchY = 3, kSubMarchZ = 4 };
 
@@ -70,6 +72,8 @@ struct Scalars {
     unsigned long long cmax_slots[kSlots];
     unsigned long long dvmax_slots[kSlots];
     unsigned long long cfl_slots[kSlots];
+    // flux protection: bad cells found by the predictor (0) and final (1) update
+    unsigned int nbad[2];
     // batched driver state (driver.f90:35-186 per box)
     double t, t_end, t_turb, dt_turb_sched;
     long long steps_done, steps_target;
@@ -84,7 +88,8 @@ struct BoxRec {
     int npass, riemann, plane_stride, nred;
     int active, recon;      // running flag; 0 PLM, 1 PPM (characteristic), 2 PLM, 3 PPM (primitive)
     int zlo, zhi;           // z planes whose cells and faces enter the step's maxima and sums
-    int tws, pad2_;         // x width of the cell tiles is 1 << tws (32, 64 or 128), height kBX >> tws
+    int tws, protect;       // x width of the cell tiles is 1 << tws (32, 64 or 128), height kBX >> tws;
+                            // protect: HLLE protection fluxes of a Roe box (flux_protection)
     int segs, segzs;        // faces per thread of the y / z sweeps 1 << segs; segzs == kSegZLog (reserved)
     double dx, cs, cour, edot, dt_turb;
     void* S[2];
@@ -95,7 +100,16 @@ struct BoxRec {
     void* mbnd;     // 6 boundary planes of unforced momentum
     double* partials;   // nred * 6 FP64 partial sums
     Scalars* sc;
+    // flux protection (protect != 0): HLLE fluxes and their corner EMFs, a
+    // per-cell bad flag and per update stage a list of up to badcap bad cells
+    void* Fp;
+    void* Ep;
+    unsigned char* bad;
+    int* badlist;
+    int badcap, pad3_;
 };
+// Flux solver of a box's scheme (4: Roe with protection fluxes).
+__host__ __device__ inline int box_solver(const BoxRec& r) { return (r.riemann == 1 && r.protect) ? 4 : r.riemann; }
 
 // A table of boxes for one set of launches.  A single box travels by value
 // in the kernel parameters (use_one); a batch is a device table with, per
@@ -119,6 +133,7 @@ struct BatchDev {
     bool any_pass = false;
     int npass_max = 0;         // largest passive count of the table
     bool any_zrange = false;   // some box restricts its maxima to a z range
+    bool any_protect = false;  // some box computes protection fluxes
     int drive_mode = 0;        // 0: no forcing, 1: every box drives (host decided), 2: per-box device flags
     int precision = 64;
     cudaStream_t st = nullptr;
