@@ -798,6 +798,24 @@ __device__ __forceinline__ T ct_bz(const T* __restrict__ S0, const T* __restrict
     return fld(S0, 9, n)[c] - dtdx * ((E[(size_t)n + c] - E[(size_t)n + cxm]) - (E[c] - E[cym]));
 }
 
+// Time-averaged velocity of the passive corrector, vel_tavg = (v_old + v_new)/2
+// (copy_velocity(.TRUE.), passive_mod.f90:227-239), written once per cell by
+// the final update (and again by the forcing kick and the protected update,
+// which change the new momentum) into three flux fields the update no longer
+// reads (the face EMF components of the x and y sweeps), so that the passive
+// corrector reads three values per cell instead of eight and divides nothing.
+// The arithmetic is that of copy_velocity: m0 * (1/rho0) and m1 * (1/rho1).
+template <class T>
+__device__ __forceinline__ T vt_of(T rho0, T m0, T rho1, T m1) {
+    const T vold = m0 * (T(1) / rho0);
+    const T irho = T(1) / rho1;
+    return T(0.5) * (vold + m1 * irho);
+}
+template <class T>
+__device__ __forceinline__ T* vt_field(const BoxRec& r, int d) {
+    return (T*)r.F + (size_t)(d == 2 ? 10 : 4 + d) * (size_t)r.n;
+}
+
 // Flux protection (flux_protection, vanleer_mod.f90:81, 2086-2202): a cell
 // whose updated density fell below MIN_DENS is flagged and listed for the
 // protection kernels of this update stage (0 predictor, 1 final).  A list
@@ -841,6 +859,7 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
     const double dx = rp.dx;
     const T asqr = (T)(rp.cs * rp.cs);
     const int do_cfl = final_stage && !sc->drive;
+    const bool write_vt = final_stage && rp.npass > 0;
     unsigned long long* cmax_slots = sc->cmax_slots;
     unsigned long long* floor_hits = &sc->floor_hits;
     unsigned int* status = &sc->status;
@@ -913,6 +932,11 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_update(BatchArg
             fld(Sout, 7, n)[c] = bx;
             fld(Sout, 8, n)[c] = by;
             fld(Sout, 9, n)[c] = bz;
+            if (write_vt) {
+                const T r0 = fld(S0, 0, n)[c];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vt_field<T>(rp, d)[c] = vt_of(r0, fld(S0, 1 + d, n)[c], out[0], out[1 + d]);
+            }
             if (do_cfl && inz)
                 cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
             if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
@@ -1010,6 +1034,7 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
     const T* __restrict__ E = (const T*)rp.E;
     const T asqr = (T)(rp.cs * rp.cs);
     const int do_cfl = final_stage && !sc->drive;
+    const bool write_vt = final_stage && rp.npass > 0;
     const int t = (int)threadIdx.x;
     const int lx = t % TW, ly = t / TW;
     int i0, j0, seg;
@@ -1131,6 +1156,10 @@ __global__ void __launch_bounds__(kTmaTile, sizeof(T) == 4 ? 6 : 1)
             fld(Sout, 7, n)[c] = bx;
             fld(Sout, 8, n)[c] = by;
             fld(Sout, 9, n)[c] = bz;
+            if (write_vt) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) vt_field<T>(rp, d)[c] = vt_of(at(0), at(1 + d), out[0], out[1 + d]);
+            }
             if (do_cfl && inz)
                 cmax = nmax(cmax, (double)cell_max_speed(out[0], out[1], out[2], out[3], bxc, byc, bzc, asqr));
             if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3]) && isfinite(bx) &&
@@ -1254,6 +1283,11 @@ __global__ void __launch_bounds__(kBX) k_prot_hydro(BatchArgs ba, double dt_scal
         }
 #pragma unroll
         for (int v = 0; v < 4; ++v) fld(Sout, v, n)[c] = out[v];
+        if (stage == 1 && rp.npass > 0) {
+            const T r0 = fld(S0, 0, n)[c];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) vt_field<T>(rp, d)[c] = vt_of(r0, fld(S0, 1 + d, n)[c], out[0], out[1 + d]);
+        }
         if (inz && !(isfinite(out[0]) && isfinite(out[1]) && isfinite(out[2]) && isfinite(out[3])))
             atomicOr(&sc->status, 2u);
     }
@@ -1452,12 +1486,16 @@ __device__ __forceinline__ T minmod(T wm, T w0, T wp) {
 // (passive_mod.f90:159-201, 227-239).  mbnd holds, on drive steps, the
 // unforced momentum of the boundary planes: [D][0] plane a = 0 and [D][1]
 // plane a = n-1 of each axis (the ghost images the reference reads).
+// The time-averaged velocity of cell c: the value the final update (or the
+// kick) stored, or, across the global boundary on a drive step, that of the
+// unforced momentum (unforced_m) computed here.
 template <class T>
-__device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict__ S1, int n, int c, int comp,
-                                   const T* unforced_m) {
+__device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict__ S1, const T* __restrict__ VT, int n,
+                                   int c, int comp, const T* unforced_m) {
+    if (!unforced_m) return VT[(size_t)(comp == 2 ? 6 : comp) * n + c];
     T vold = vel_of(S0, n, c, comp);
     T irho = T(1) / fld(S1, 0, n)[c];
-    T m1 = unforced_m ? *unforced_m : fld(S1, 1 + comp, n)[c];
+    T m1 = *unforced_m;
     return T(0.5) * (vold + m1 * irho);
 }
 
@@ -1476,6 +1514,7 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
     const T* __restrict__ S0 = (const T*)rp.S[0];
     T* __restrict__ S1 = (T*)rp.S[1];
     const T* __restrict__ SH = (const T*)rp.SH;
+    const T* __restrict__ VT = vt_field<T>(rp, 0);   // fields 0, 1 at +0, +n; field 2 at +6n (vt_field)
     const double dx = rp.dx;
     const int drive = sc->drive;
     const T* __restrict__ mbnd = (const T*)rp.mbnd;
@@ -1503,8 +1542,8 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
     // k-2..k+1 and the minmod slopes at k-1, k
     const int km = wrap_dn(k0, dm.nz);
     const int ckm = r0 + km * plane, ck0 = r0 + k0 * plane;
-    T vz_m = vtavg(S0, S1, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
-    T vz_0 = vtavg(S0, S1, n, ck0, 2, (const T*)nullptr);
+    T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
+    T vz_0 = vtavg(S0, S1, VT, n, ck0, 2, (const T*)nullptr);
     T s_m[NP], s_0[NP], s_p[NP], dl_m[NP], dl_0[NP];
     {
         const int ckm2 = r0 + wrap_any(k0 - 2, dm.nz) * plane, ckp = r0 + wrap_up(k0, dm.nz) * plane;
@@ -1526,13 +1565,13 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
         const int cxm = rxm + k * plane, cxp = rxp + k * plane, cxm2 = rxm2 + k * plane, cxp2 = rxp2 + k * plane;
         const int cym = rym + k * plane, cyp = ryp + k * plane, cym2 = rym2 + k * plane, cyp2 = ryp2 + k * plane;
         const int pofs_x = j + dm.ny * k, pofs_y = i + dm.nx * k;
-        const T vx0 = vtavg(S0, S1, n, c, 0, (const T*)nullptr);
-        const T vy0 = vtavg(S0, S1, n, c, 1, (const T*)nullptr);
-        const T vxm = vtavg(S0, S1, n, cxm, 0, um_x ? um_x + pofs_x : (const T*)nullptr);
-        const T vxp = vtavg(S0, S1, n, cxp, 0, up_x ? up_x + pofs_x : (const T*)nullptr);
-        const T vym = vtavg(S0, S1, n, cym, 1, um_y ? um_y + pofs_y : (const T*)nullptr);
-        const T vyp = vtavg(S0, S1, n, cyp, 1, up_y ? up_y + pofs_y : (const T*)nullptr);
-        const T vz_p = vtavg(S0, S1, n, czp, 2, (k == dm.nz - 1) ? up_z : (const T*)nullptr);
+        const T vx0 = vtavg(S0, S1, VT, n, c, 0, (const T*)nullptr);
+        const T vy0 = vtavg(S0, S1, VT, n, c, 1, (const T*)nullptr);
+        const T vxm = vtavg(S0, S1, VT, n, cxm, 0, um_x ? um_x + pofs_x : (const T*)nullptr);
+        const T vxp = vtavg(S0, S1, VT, n, cxp, 0, up_x ? up_x + pofs_x : (const T*)nullptr);
+        const T vym = vtavg(S0, S1, VT, n, cym, 1, um_y ? um_y + pofs_y : (const T*)nullptr);
+        const T vyp = vtavg(S0, S1, VT, n, cyp, 1, up_y ? up_y + pofs_y : (const T*)nullptr);
+        const T vz_p = vtavg(S0, S1, VT, n, czp, 2, (k == dm.nz - 1) ? up_z : (const T*)nullptr);
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
             if (p >= npass) break;
@@ -1569,6 +1608,200 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
         }
         vz_m = vz_0;
         vz_0 = vz_p;
+    }
+}
+
+// ------------------------------------------------------ passive corrector, bulk-copy fed
+// The same corrector for single boxes whose rows are whole 128-cell tiles: a
+// block owns a 128-cell segment of row j and walks kSegZ planes; lanes of
+// warp 0 stream each plane's x/y stencil into shared memory with bulk
+// asynchronous copies one plane ahead (two stages, mbarrier completion, as
+// k_update_tma): per scalar the half-step rows j-2..j+2 (row j with 16-byte
+// halo segments on both sides, for the x neighbours out to i +- 2) and the
+// step-start row j; the time-averaged v_x of row j (halos on both sides) and
+// v_y of rows j-1, j, j+1; and the new values of the z stencil, row j of each
+// scalar at plane k+2 and of v_z at plane k+1 (the rest of the z stencil is
+// carried).  On drive steps the neighbours
+// across the global boundary take the unforced momentum (mbnd) as in
+// k_passive_corr.  Waits are bounded (IMHD_S_WAIT on time-out).
+template <class T, int NP>
+constexpr int ptma_rows() { return 7 * NP + 5; }
+template <class T>
+constexpr int ptma_row_stride() { return kTmaTile + 2 * (16 / (int)sizeof(T)); }
+template <class T, int NP>
+constexpr size_t ptma_stage_bytes() {
+    return ((size_t)ptma_rows<T, NP>() * ptma_row_stride<T>() * sizeof(T) + 127) / 128 * 128;
+}
+template <class T, int NP>
+constexpr size_t passive_tma_smem_bytes() { return 2 * ptma_stage_bytes<T, NP>(); }
+
+__host__ __device__ __forceinline__ bool passive_by_tma(int nx) { return nx % kTmaTile == 0; }
+
+template <class T, int NP>
+__global__ void __launch_bounds__(kTmaTile, 8) k_passive_corr_tma(BatchArgs ba) {
+    extern __shared__ __align__(128) unsigned char ptma_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    const BoxRec rp = ba.one;
+    Scalars* sc = rp.sc;
+    const int npass = rp.npass;
+    if (!rp.active || npass == 0) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S0 = (const T*)rp.S[0];
+    T* __restrict__ S1 = (T*)rp.S[1];
+    const T* __restrict__ SH = (const T*)rp.SH;
+    const T* __restrict__ VT = vt_field<T>(rp, 0);   // v_x, v_y at +0, +n; v_z at +6n
+    const int drive = sc->drive;
+    const T* __restrict__ mbnd = (const T*)rp.mbnd;
+    const int plane_stride = rp.plane_stride;
+    constexpr int HE = 16 / (int)sizeof(T);
+    constexpr int RS = ptma_row_stride<T>();
+    const int t = (int)threadIdx.x;
+    const int i0 = (int)blockIdx.x * kTmaTile, j = (int)blockIdx.y, seg = (int)blockIdx.z;
+    const int i = i0 + t;
+    const int k0 = seg * kSegZ, k1 = min(k0 + kSegZ, dm.nz);
+    const int n = dm.n, plane = dm.nx * dm.ny;
+    const T dtdx = (T)(sc->dt / rp.dx);
+    const int nrows = 7 * npass + 5;
+    const int ih = (i0 == 0 ? dm.nx : i0) - HE;       // left halo: cells i0-HE .. i0-1
+    const int ir = (i0 + kTmaTile) % dm.nx;            // right halo: cells i0+128 .. i0+128+HE-1
+    if (t == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    // rows of plane k into stage g: scalar p: SH rows j-2..j+2 at 6p..6p+4,
+    // step-start row j at 6p+5; then v_x row j, v_y rows j-1, j, j+1
+    auto issue = [&](int g, int k) {
+        T* rows = (T*)(ptma_smem + (size_t)g * ptma_stage_bytes<T, NP>());
+        unsigned long long* bar = &bars[g];
+        if (t == 0)
+            mbar_expect_tx(bar, (unsigned)(nrows * kTmaTile * (int)sizeof(T) + (2 * npass + 2) * 16));
+        __syncwarp();
+        for (int R = t; R < nrows; R += 32) {
+            const T* base;
+            int jr = j, kr = k;
+            bool halo = false;
+            if (R < 6 * npass) {
+                const int p = R / 6, q = R % 6;
+                if (q < 5) { base = fld(SH, p, n); jr = wrap_any(j + q - 2, dm.ny); halo = (q == 2); }
+                else base = fld(S0, 10 + p, n);
+            } else if (R < 6 * npass + 4) {
+                const int q = R - 6 * npass;
+                if (q == 0) { base = VT; halo = true; }
+                else { base = VT + (size_t)n; jr = wrap_any(j + q - 2, dm.ny); }
+            } else if (R < 7 * npass + 4) {   // the z stencil's new values: scalar p at k+2, v_z at k+1
+                base = fld(SH, R - 6 * npass - 4, n);
+                kr = wrap_any(k + 2, dm.nz);
+            } else {
+                base = VT + (size_t)6 * n;
+                kr = wrap_up(k, dm.nz);
+            }
+            const size_t ofs = (size_t)dm.nx * (jr + (size_t)dm.ny * kr);
+            bulk_g2s(rows + R * RS + HE, base + i0 + ofs, kTmaTile * (unsigned)sizeof(T), bar);
+            if (halo) {
+                bulk_g2s(rows + R * RS, base + ih + ofs, 16u, bar);
+                bulk_g2s(rows + R * RS + HE + kTmaTile, base + ir + ofs, 16u, bar);
+            }
+        }
+    };
+    if (t < 32) issue(0, k0);
+
+    const int r0 = i + dm.nx * j;
+    // drive steps: the velocity across the global boundary of each axis uses
+    // the unforced momentum of the ghost image (mbnd planes, see k_force_kick)
+    const T* um_x = (drive && i == 0) ? mbnd + (size_t)1 * plane_stride : nullptr;
+    const T* up_x = (drive && i == dm.nx - 1) ? mbnd + (size_t)0 * plane_stride : nullptr;
+    const T* um_y = (drive && j == 0) ? mbnd + (size_t)3 * plane_stride : nullptr;
+    const T* up_y = (drive && j == dm.ny - 1) ? mbnd + (size_t)2 * plane_stride : nullptr;
+    const T* um_z = drive ? mbnd + (size_t)5 * plane_stride + r0 : nullptr;
+    const T* up_z = drive ? mbnd + (size_t)4 * plane_stride + r0 : nullptr;
+    const int rxm = wrap_dn(i, dm.nx) + dm.nx * j, rxp = wrap_up(i, dm.nx) + dm.nx * j;
+    const int rym = i + dm.nx * wrap_dn(j, dm.ny), ryp = i + dm.nx * wrap_up(j, dm.ny);
+    // z window of the column: v_z at k-1, k; scalars at k-1..k+1 and the
+    // minmod slopes at k-1, k
+    const int km = wrap_dn(k0, dm.nz);
+    const int ckm = r0 + km * plane, ck0 = r0 + k0 * plane;
+    T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
+    T vz_0 = vtavg(S0, S1, VT, n, ck0, 2, (const T*)nullptr);
+    T s_m[NP], s_0[NP], s_p[NP], dl_m[NP], dl_0[NP];
+    {
+        const int ckm2 = r0 + wrap_any(k0 - 2, dm.nz) * plane, ckp = r0 + wrap_up(k0, dm.nz) * plane;
+#pragma unroll
+        for (int p = 0; p < NP; ++p)
+            if (p < npass) {
+                const T* s = fld(SH, p, n);
+                const T sm2 = s[ckm2];
+                s_m[p] = s[ckm];
+                s_0[p] = s[ck0];
+                s_p[p] = s[ckp];
+                dl_m[p] = minmod(sm2, s_m[p], s_0[p]);
+                dl_0[p] = minmod(s_m[p], s_0[p], s_p[p]);
+            }
+    }
+    bool ok = true;
+    for (int k = k0; k < k1; ++k) {
+        const int it = k - k0, g = it & 1;
+        if (t < 32 && k + 1 < k1) issue(g ^ 1, k + 1);
+        if (ok && !mbar_wait(&bars[g], (unsigned)((it >> 1) & 1))) {
+            ok = false;
+            atomicOr(&sc->status, kStatusWait);
+        }
+        if (ok) {
+            const T* rows = (const T*)(ptma_smem + (size_t)g * ptma_stage_bytes<T, NP>()) + HE + t;
+            auto at = [&](int R, int dx) { return rows[R * RS + dx]; };
+            const int c = r0 + k * plane;
+            const int czp = r0 + wrap_up(k, dm.nz) * plane;
+            const int vx_row = 6 * npass, vy_row = 6 * npass + 1;
+            const T vx0 = at(vx_row, 0), vy0 = at(vy_row + 1, 0);
+            const T vxm = um_x ? vtavg(S0, S1, VT, n, rxm + k * plane, 0, um_x + (j + dm.ny * k)) : at(vx_row, -1);
+            const T vxp = up_x ? vtavg(S0, S1, VT, n, rxp + k * plane, 0, up_x + (j + dm.ny * k)) : at(vx_row, 1);
+            const T vym = um_y ? vtavg(S0, S1, VT, n, rym + k * plane, 1, um_y + (i + dm.nx * k)) : at(vy_row, 0);
+            const T vyp = up_y ? vtavg(S0, S1, VT, n, ryp + k * plane, 1, up_y + (i + dm.nx * k)) : at(vy_row + 2, 0);
+            const T vz_p = (drive && k == dm.nz - 1) ? vtavg(S0, S1, VT, n, czp, 2, up_z) : at(7 * npass + 4, 0);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                if (p >= npass) break;
+                const int rj = 6 * p + 2;      // row j of scalar p
+                const T s0 = s_0[p];
+                T dF[3];
+                {
+                    const T sm = at(rj, -1), sp = at(rj, 1), sm2 = at(rj, -2), sp2 = at(rj, 2);
+                    const T dlm = minmod(sm2, sm, s0), dl0 = minmod(sm, s0, sp), dlp = minmod(s0, sp, sp2);
+                    const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vx0 + vxp));
+                    const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vxm + vx0));
+                    dF[0] = Fp - Fm;
+                }
+                {
+                    const T sm = at(rj - 1, 0), sp = at(rj + 1, 0), sm2 = at(rj - 2, 0), sp2 = at(rj + 2, 0);
+                    const T dlm = minmod(sm2, sm, s0), dl0 = minmod(sm, s0, sp), dlp = minmod(s0, sp, sp2);
+                    const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vy0 + vyp));
+                    const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vym + vy0));
+                    dF[1] = Fp - Fm;
+                }
+                {
+                    const T sm = s_m[p], sp = s_p[p], sp2 = at(6 * npass + 4 + p, 0);
+                    const T dlm = dl_m[p], dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
+                    const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vz_0 + vz_p));
+                    const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vz_m + vz_0));
+                    dF[2] = Fp - Fm;
+                    s_m[p] = s0;
+                    s_0[p] = sp;
+                    s_p[p] = sp2;
+                    dl_m[p] = dl0;
+                    dl_0[p] = dlp;
+                }
+                fld(S1, 10 + p, n)[c] = at(6 * p + 5, 0) - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
+            }
+            vz_m = vz_0;
+            vz_0 = vz_p;
+        }
+        __syncthreads();   // every thread is done with stage g before it is refilled
+    }
+    // a wait that gave up may leave copies in flight: let them land (bounded) before exit
+    if (t == 0 && !ok) {
+        const int last = k1 - 1 - k0;
+        mbar_wait(&bars[last & 1], (unsigned)((last >> 1) & 1));
     }
 }
 
@@ -1725,6 +1958,12 @@ __global__ void __launch_bounds__(kBX) k_force_kick(BatchArgs ba) {
         fld(S1, 1, n)[c] = mx;
         fld(S1, 2, n)[c] = my;
         fld(S1, 3, n)[c] = mz;
+        if (save_bnd) {   // the time-averaged velocity of the kicked momentum
+            const T rho0 = fld(S0, 0, n)[c], rho1 = fld(S1, 0, n)[c];
+            vt_field<T>(rp, 0)[c] = vt_of(rho0, fld(S0, 1, n)[c], rho1, mx);
+            vt_field<T>(rp, 1)[c] = vt_of(rho0, fld(S0, 2, n)[c], rho1, my);
+            vt_field<T>(rp, 2)[c] = vt_of(rho0, fld(S0, 3, n)[c], rho1, mz);
+        }
         if (inz) dvmax = vmax(vmax(vmax(dvmax, fabs(dmx) / r0), fabs(dmy) / r0), fabs(dmz) / r0);
         if (inz) cmax = (double)cell_max_speed(fld(S1, 0, n)[c], mx, my, mz, fld(S1, 4, n)[c], fld(S1, 5, n)[c],
                                       fld(S1, 6, n)[c], asqr);

@@ -79,7 +79,8 @@ def test_fp64_bit_exact_32_roe():
 # neighbours from the periodic images.
 @pytest.mark.parametrize("riemann,n,npass", [("roe", (128, 12, 20), 1), ("hlld", (256, 12, 18), 2),
                                              ("hlle", (256, 12, 18), 4), ("roe", (128, 12, 18), 0),
-                                             ("hlld", (64, 12, 18), 1), ("roe", (192, 14, 17), 2)])
+                                             ("hlld", (64, 12, 18), 1), ("roe", (192, 14, 17), 2),
+                                             ("roe", (128, 12, 16), 5)])
 def test_fp64_bit_exact_tma_update_rows(riemann, n, npass):
     ic = problems.smooth_wave_box(n, npass=max(npass, 1))
     if npass == 0:
@@ -92,10 +93,16 @@ def test_fp64_bit_exact_tma_update_rows(riemann, n, npass):
     assert_exact(g, o)
 
 
-def test_fp64_tma_update_rows_driven():
+@pytest.mark.parametrize("npass", [1, 3])
+def test_fp64_tma_update_rows_driven(npass):
+    # drive steps: the bulk-copy fed passive corrector takes the unforced
+    # momentum across the global boundary (x, y and z faces)
     from oracle.pyoracle import Oracle
     n = (128, 12, 18)
     ic = problems.smooth_wave_box(n, npass=1)
+    if npass > 1:
+        rng = np.random.default_rng(3)
+        ic = (ic[0], ic[1], rng.uniform(0.0, 1.0, (npass,) + ic[2].shape[1:]))
     gen = Oracle(n, riemann="roe", npass=1)
     delv = gen.generate_ref_force(seeds=(1234, 5678, 9123))
     gen.close()
