@@ -204,9 +204,9 @@ def stage_bytes(esz, npass):
         "pred_update": 32 * esz,          # 7 state + 12 fluxes + 3 EMFs in; 10 fields out
         "corr_flux_x": 13 * esz, "corr_flux_y": 13 * esz, "corr_flux_z": 13 * esz,
         "corr_emf": 16 * esz,
-        "final_update": 32 * esz,
+        "final_update": 35 * esz,         # and the passive corrector's 3 time-averaged velocities out
         "passive_pred": (4 + 2 * npass) * esz,
-        "passive_corr": (8 + 3 * npass) * esz,
+        "passive_corr": (3 + 3 * npass) * esz,   # 3 velocities, half-step and step-start scalars in; scalars out
         "force_sums": 7 * esz, "force_kick": 12 * esz, "finalize": 0,
     }
 
@@ -392,7 +392,8 @@ def run_ours(a, ws, rank, local):
     for kname, sts in KERNEL_STAGES.items():
         ms = [per_stage[st]["ms_per_launch"] for st in sts if st in per_stage]
         if ms:
-            kernels[kname] = (sum(ms), sum(ms) / len(ms), sb[sts[0]])
+            nb = [sb[st] for st in sts if st in per_stage]
+            kernels[kname] = (sum(ms), sum(ms) / len(ms), sum(nb) / len(nb))
     for name, v in per_stage.items():
         if name not in grouped:
             kernels[name] = (v["ms_per_launch"], v["ms_per_launch"], sb.get(name, 0))

@@ -305,11 +305,12 @@ void imhd_batch_destroy(imhd_batch* batch);
 /* ---- serving: a request loop with continuous batching -------------------
  * imhd_server_start launches a worker thread that owns one device.  Requests
  * (a box solve: configuration, step count, initial condition, forcing) are
- * queued by imhd_server_submit from any host thread; the worker admits them
- * in arrival order while their device bytes fit hbm_budget_bytes (and, if
- * max_resident_cells > 0, while the resident cells stay under it), builds
- * each box on the device, and advances all resident boxes together with the
- * batched step (per-box clocks as in imhd_batch_*).  Every steps_per_round
+ * queued by imhd_server_submit from any host thread; a builder thread admits
+ * them in arrival order while their device bytes fit hbm_budget_bytes (and,
+ * if max_resident_cells > 0, while the resident cells stay under it) and
+ * builds each box on the device while the worker steps, and the worker
+ * advances all resident boxes together with the batched step (per-box clocks
+ * as in imhd_batch_*).  Every steps_per_round
  * replays it retires finished boxes (result copied to host memory, device
  * memory freed) and admits waiting ones, so requests that arrive while others
  * run join the running batch.  A box's result does not depend on what else
@@ -367,12 +368,13 @@ int imhd_server_poll(imhd_server* server, long long id, int* state, double* q, d
                      double* info);
 /* {queued, resident, admitted, completed, failed, graph replays, kernel
  * launches, table rebuilds, resident bytes, peak resident bytes, peak
- * resident boxes, then seconds the worker spent building admitted boxes,
- * rebuilding the table and graph, stepping, reading clocks and retiring, and
- * seconds the harvester spent downloading results}; n >= IMHD_SERVER_NSTATS.
- * Finished boxes are downloaded by a second thread on a stream of their own
- * while the step loop goes on; their memory counts against the budget until
- * the download ends. */
+ * resident boxes, then seconds the builder spent building admitted boxes,
+ * seconds the worker spent rebuilding the table and graph, stepping, reading
+ * clocks and retiring, and seconds the harvester spent downloading results};
+ * n >= IMHD_SERVER_NSTATS.  Admitted boxes are built by a builder thread on a
+ * stream of its own, and finished boxes downloaded by a harvester thread on
+ * another, while the step loop goes on; a box's memory counts against the
+ * budget from its admission until its download ends. */
 int imhd_server_stats(imhd_server* server, double* out, int n);
 /* Stop the worker: drain != 0 finishes every queued and running request
  * first, drain == 0 cancels them.  Results stay pollable until destroy. */

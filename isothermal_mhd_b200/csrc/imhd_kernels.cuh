@@ -525,10 +525,11 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
 // exactly once (the tiled kernel above recomputes slopes at tile edges and
 // stages a halo).  PPM evaluates the edges of cells i and i+1 per face.
 // Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
-// FP32: four 256-thread blocks per SM (64 registers): 3.8 -> 3.4 ms (Roe,
-// PLM) at 512^3.
+// FP32: 64 registers; eight 128-thread blocks per SM (smaller barrier
+// groups, 27 KB of shared memory each at nx = 512): 3.45 -> 3.19 ms (Roe,
+// PLM) at 512^3 against four 256-thread blocks.
 template <class T, int SCHEME, bool ONE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 1) k_corr_flux_xrow(BatchArgs ba) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 1) k_corr_flux_xrow(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     constexpr int RECON = scheme_recon(SCHEME);
     constexpr bool PPM = (RECON & 1) != 0, PRIM = (RECON & 2) != 0;
@@ -774,6 +775,167 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(Batc
         a010 = a011;
         fx2_000 = fx2_001;
         fy1_000 = fy1_001;
+    }
+}
+
+// ------------------------------------------- corner EMF, shared cell-centre values
+// The corner EMFs of a single box whose rows are whole 32-cell segments and
+// whose y edge is a multiple of 8: a block owns a 32 x 8 tile of columns and
+// walks kEmfSegZ planes.  Each plane's cell-centre EMFs and velocities are
+// computed once per cell into a three-plane ring in shared memory (a ninth
+// warp computes the tile's +y row and +x column), and the corners read their
+// neighbours' values from there; the z-column kernel above computes each
+// cell's values three times and one component a fourth.  The same operations
+// on the same operands: the results are those of k_corner_emf.  One barrier
+// per plane: plane k+1 goes to the slot of plane k-2, which every thread
+// finished reading before it arrived at the barrier of plane k-1.
+constexpr int kEmfTX = 32, kEmfTY = 8, kEmfSegZ = 32;
+constexpr int kEmfThreads = kEmfTX * (kEmfTY + 1);
+__host__ __device__ __forceinline__ bool emf_by_tiles(int nx, int ny) {
+    return nx % kEmfTX == 0 && ny % kEmfTY == 0;
+}
+
+template <class T>
+struct EmfRing {                       // [slot][ux, uy, ex, ey, ez][row][column]
+    T v[3][5][kEmfTY + 1][kEmfTX + 1];
+};
+template <class T>
+__device__ __forceinline__ void ring_put(EmfRing<T>& R, int s, int y, int x, const CellEV<T>& a) {
+    R.v[s][0][y][x] = a.ux;
+    R.v[s][1][y][x] = a.uy;
+    R.v[s][2][y][x] = a.ex;
+    R.v[s][3][y][x] = a.ey;
+    R.v[s][4][y][x] = a.ez;
+}
+
+template <class T, bool PROT = false>
+__global__ void __launch_bounds__(kEmfThreads, sizeof(T) == 4 ? 3 : 1) k_corner_emf_tile(BatchArgs ba,
+                                                                                           int half_step_state) {
+    __shared__ EmfRing<T> ring;
+    const BoxRec rp = ba.one;
+    if (!rp.active || (PROT && !rp.protect)) return;
+    const Dims dm = dims_of(rp);
+    const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
+    const T* __restrict__ F = (const T*)(PROT ? rp.Fp : rp.F);
+    T* __restrict__ E = (T*)(PROT ? rp.Ep : rp.E);
+    const int lx = (int)threadIdx.x & 31, ly = (int)threadIdx.x >> 5;   // ly == kEmfTY: the halo warp
+    const int i0 = (int)blockIdx.x * kEmfTX, j0 = (int)blockIdx.y * kEmfTY;
+    const int k0 = (int)blockIdx.z * kEmfSegZ, k1 = min(k0 + kEmfSegZ, dm.nz);
+    const int n = dm.n, plane = dm.nx * dm.ny;
+    const bool out = ly < kEmfTY;
+    // the cells whose values this thread computes per plane: its own column
+    // (a halo-warp lane: row j0+8) and, lanes 0..8 of the halo warp, rows
+    // j0..j0+8 of column i0+32 (periodic images at the box edges)
+    const int jh = (j0 + kEmfTY == dm.ny) ? 0 : j0 + kEmfTY;
+    const int ih = (i0 + kEmfTX == dm.nx) ? 0 : i0 + kEmfTX;
+    const int ra = i0 + lx + dm.nx * (out ? j0 + ly : jh);
+    const bool second = !out && lx <= kEmfTY;
+    const int rb = ih + dm.nx * (lx == kEmfTY ? jh : j0 + lx);
+    const int ya = out ? ly : kEmfTY;
+    // corner neighbours of an output column
+    const int i = i0 + lx, j = j0 + (out ? ly : 0);
+    const int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny);
+    const int r000 = i + dm.nx * j, r100 = ip + dm.nx * j, r010 = i + dm.nx * jp;
+    const T* Fx_bt1 = F + (size_t)4 * n;
+    const T* Fx_bt2 = F + (size_t)5 * n;
+    const T* Fy_bt1 = F + (size_t)10 * n;
+    const T* Fy_bt2 = F + (size_t)11 * n;
+    const T* Fz_bt1 = F + (size_t)16 * n;
+    const T* Fz_bt2 = F + (size_t)17 * n;
+    int s0 = 0;
+    CellEV<T> own = cell_ev(S, n, ra + k0 * plane);
+    ring_put(ring, s0, ya, lx, own);
+    if (second) ring_put(ring, s0, lx, kEmfTX, cell_ev(S, n, rb + k0 * plane));
+    T fx2_000 = T(0), fy1_000 = T(0);
+    if (out) {
+        fx2_000 = Fx_bt2[r000 + k0 * plane];
+        fy1_000 = Fy_bt1[r000 + k0 * plane];
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int kp = wrap_up(k, dm.nz);
+        const int s1 = (s0 == 2) ? 0 : s0 + 1;
+        const CellEV<T> nxt = cell_ev(S, n, ra + kp * plane);
+        ring_put(ring, s1, ya, lx, nxt);
+        if (second) ring_put(ring, s1, lx, kEmfTX, cell_ev(S, n, rb + kp * plane));
+        __syncthreads();
+        if (out) {
+            const int c000 = r000 + k * plane, c100 = r100 + k * plane, c010 = r010 + k * plane;
+            const int c001 = r000 + kp * plane;
+            const auto& A = ring.v[s0];
+            const auto& B = ring.v[s1];
+            const T x_ux = A[0][ly][lx + 1], x_ey = A[3][ly][lx + 1], x_ez = A[4][ly][lx + 1];
+            const T y_uy = A[1][ly + 1][lx], y_ex = A[2][ly + 1][lx], y_ez = A[4][ly + 1][lx];
+            const T xy_ez = A[4][ly + 1][lx + 1];
+            const T xp_ey = B[3][ly][lx + 1], yp_ex = B[2][ly + 1][lx];
+            const T fx2_001 = Fx_bt2[c001], fy1_001 = Fy_bt1[c001];
+            const T vx = T(0.5) * (own.ux + x_ux);
+            const T vy = T(0.5) * (own.uy + y_uy);
+            const T vz = T(0.5) * (own.uz + nxt.uz);
+            // Ez at (i+1/2, j+1/2, k)
+            {
+                T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
+                T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
+                T E33_000 = own.ez, E33_100 = x_ez, E33_010 = y_ez, E33_110 = xy_ez;
+                T dyL14 = T(2) * (E32_000 - E33_000);
+                T dyR14 = T(2) * (E32_100 - E33_100);
+                T dyL34 = T(2) * (E33_010 - E32_000);
+                T dyR34 = T(2) * (E33_110 - E32_100);
+                T dy1214, dy1234;
+                upwind_pair(vx, dyL14, dyR14, dyL34, dyR34, dy1214, dy1234);
+                T dxL14 = T(2) * (E31_000 - E33_000);
+                T dxR14 = T(2) * (E31_010 - E33_010);
+                T dxL34 = T(2) * (E33_100 - E31_000);
+                T dxR34 = T(2) * (E33_110 - E31_010);
+                T dx1412, dx3412;
+                upwind_pair(vy, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+                E[(size_t)2 * n + c000] = T(0.25) * (E31_000 + E31_010 + E32_000 + E32_100) +
+                                          T(0.125) * ((dy1214 - dy1234) + (dx1412 - dx3412));
+            }
+            // Ey at (i+1/2, j, k+1/2)
+            {
+                T E21_000 = fx2_000, E21_001 = fx2_001;
+                T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
+                T E23_000 = own.ey, E23_100 = x_ey, E23_001 = nxt.ey, E23_101 = xp_ey;
+                T dzL14 = T(2) * (E22_000 - E23_000);
+                T dzR14 = T(2) * (E22_100 - E23_100);
+                T dzL34 = T(2) * (E23_001 - E22_000);
+                T dzR34 = T(2) * (E23_101 - E22_100);
+                T dz1214, dz1234;
+                upwind_pair(vx, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+                T dxL14 = T(2) * (E21_000 - E23_000);
+                T dxR14 = T(2) * (E21_001 - E23_001);
+                T dxL34 = T(2) * (E23_100 - E21_000);
+                T dxR34 = T(2) * (E23_101 - E21_001);
+                T dx1412, dx3412;
+                upwind_pair(vz, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
+                E[(size_t)1 * n + c000] = T(0.25) * (E21_000 + E21_001 + E22_000 + E22_100) +
+                                          T(0.125) * ((dz1214 - dz1234) + (dx1412 - dx3412));
+            }
+            // Ex at (i, j+1/2, k+1/2)
+            {
+                T E11_000 = -fy1_000, E11_001 = -fy1_001;
+                T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
+                T E13_000 = own.ex, E13_010 = y_ex, E13_001 = nxt.ex, E13_011 = yp_ex;
+                T dzL14 = T(2) * (E12_000 - E13_000);
+                T dzR14 = T(2) * (E12_010 - E13_010);
+                T dzL34 = T(2) * (E13_001 - E12_000);
+                T dzR34 = T(2) * (E13_011 - E12_010);
+                T dz1214, dz1234;
+                upwind_pair(vy, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
+                T dyL14 = T(2) * (E11_000 - E13_000);
+                T dyR14 = T(2) * (E11_001 - E13_001);
+                T dyL34 = T(2) * (E13_010 - E11_000);
+                T dyR34 = T(2) * (E13_011 - E11_001);
+                T dy1412, dy3412;
+                upwind_pair(vz, dyL14, dyR14, dyL34, dyR34, dy1412, dy3412);
+                E[c000] = T(0.25) * (E11_000 + E11_001 + E12_000 + E12_010) +
+                          T(0.125) * ((dz1214 - dz1234) + (dy1412 - dy3412));
+            }
+            fx2_000 = fx2_001;
+            fy1_000 = fy1_001;
+        }
+        own = nxt;
+        s0 = s1;
     }
 }
 
@@ -1399,11 +1561,18 @@ __global__ void __launch_bounds__(kBX) k_prot_clear(BatchArgs ba, int stage) {
 }
 
 // ============================================================ passive scalars
-// Upwind flux of compute_fluxes_1d (passive_mod.f90:594-627).
+// Upwind flux of compute_fluxes_1d (passive_mod.f90:594-627).  FP64 keeps
+// the reference's form; FP32 selects the upwind state, which equals it for
+// finite operands (0.5 * (2 * u + 0 * v) = u) in two instructions instead of
+// six.
 template <class T>
 __device__ __forceinline__ T upwind_flux(T uL, T uR, T vavg) {
-    T theta = (vavg >= T(0)) ? T(1) : T(-1);
-    return T(0.5) * ((T(1) + theta) * uL + (T(1) - theta) * uR);
+    if constexpr (sizeof(T) == 4) {
+        return (vavg >= T(0)) ? uL : uR;
+    } else {
+        T theta = (vavg >= T(0)) ? T(1) : T(-1);
+        return T(0.5) * ((T(1) + theta) * uL + (T(1) - theta) * uR);
+    }
 }
 template <class T>
 __device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int comp) {
@@ -1414,8 +1583,9 @@ __device__ __forceinline__ T vel_of(const T* __restrict__ S, int n, int c, int c
 // Predictor: s_h = s - (dt/2dx) sum_d v_d (F_d(i+1/2) - F_d(i-1/2)) with
 // first-order upwind fluxes and the step-start velocity (passive_mod.f90:
 // 133-157, 204-224, 562-590).
-// A thread walks a column of kSegZ cells along z, carrying the z-neighbour
-// velocities and scalars of the previous cell.  The neighbour loads are
+// A thread walks a column of kSegZ cells along z, carrying the z velocity
+// and the flux through the lower z face (the upper face's of the previous
+// cell: the same operands).  The neighbour loads are
 // latency-bound, so FP32 with up to four scalars runs eight blocks per SM
 // (64 registers).
 template <class T, bool ONE, int NP>
@@ -1440,14 +1610,17 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
     const int rym = i + dm.nx * wrap_dn(j, dm.ny), ryp = i + dm.nx * wrap_up(j, dm.ny);
     // z neighbours of the first cell
     const int ckm = r0 + wrap_dn(k0, dm.nz) * plane, ck0 = r0 + k0 * plane;
-    T vz_m = vel_of(S0, n, ckm, 2), vz_0 = vel_of(S0, n, ck0, 2);
-    T s_m[NP], s_0[NP];
+    T vz_0 = vel_of(S0, n, ck0, 2);
+    T s_0[NP], fz_m[NP];
+    {
+        const T vz_m = vel_of(S0, n, ckm, 2);
 #pragma unroll
-    for (int p = 0; p < NP; ++p)
-        if (p < npass) {
-            s_m[p] = fld(S0, 10 + p, n)[ckm];
-            s_0[p] = fld(S0, 10 + p, n)[ck0];
-        }
+        for (int p = 0; p < NP; ++p)
+            if (p < npass) {
+                s_0[p] = fld(S0, 10 + p, n)[ck0];
+                fz_m[p] = upwind_flux(fld(S0, 10 + p, n)[ckm], s_0[p], T(0.5) * (vz_m + vz_0));
+            }
+    }
     for (int k = k0; k < k1; ++k) {
         const int c = r0 + k * plane, czp = r0 + wrap_up(k, dm.nz) * plane;
         const int cxm = rxm + k * plane, cxp = rxp + k * plane, cym = rym + k * plane, cyp = ryp + k * plane;
@@ -1463,12 +1636,12 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
             T dF[3];
             dF[0] = upwind_flux(s0, s[cxp], T(0.5) * (vx0 + vxp)) - upwind_flux(s[cxm], s0, T(0.5) * (vxm + vx0));
             dF[1] = upwind_flux(s0, s[cyp], T(0.5) * (vy0 + vyp)) - upwind_flux(s[cym], s0, T(0.5) * (vym + vy0));
-            dF[2] = upwind_flux(s0, s_zp, T(0.5) * (vz_0 + vz_p)) - upwind_flux(s_m[p], s0, T(0.5) * (vz_m + vz_0));
+            const T fz_p = upwind_flux(s0, s_zp, T(0.5) * (vz_0 + vz_p));
+            dF[2] = fz_p - fz_m[p];
             fld(SH, p, n)[c] = s0 - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
-            s_m[p] = s0;
             s_0[p] = s_zp;
+            fz_m[p] = fz_p;
         }
-        vz_m = vz_0;
         vz_0 = vz_p;
     }
 }
@@ -1500,7 +1673,8 @@ __device__ __forceinline__ T vtavg(const T* __restrict__ S0, const T* __restrict
 }
 
 // A thread walks a column of kSegZ cells along z, carrying the z-neighbour
-// time-averaged velocities, half-step scalars and their minmod slopes.
+// time-averaged velocity, half-step scalars, their minmod slopes and the
+// flux through the lower z face (the upper face's of the previous cell).
 // Eight blocks per SM in FP32 with up to four scalars, as k_passive_pred
 // (a few spilled values cost less than the lost occupancy).
 template <class T, bool ONE, int NP>
@@ -1538,25 +1712,26 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
     const T* up_y = (drive && j == dm.ny - 1) ? mbnd + (size_t)2 * plane_stride : nullptr;
     const T* um_z = drive ? mbnd + (size_t)5 * plane_stride + (i + dm.nx * j) : nullptr;
     const T* up_z = drive ? mbnd + (size_t)4 * plane_stride + (i + dm.nx * j) : nullptr;
-    // z neighbours of the first cell: velocities at k-1, k; scalars at
-    // k-2..k+1 and the minmod slopes at k-1, k
+    // z neighbours of the first cell: velocity at k; scalars at k, k+1, the
+    // minmod slope at k and the flux through the face k-1/2 (from the
+    // velocities at k-1, k, the scalars at k-2..k+1 and the slopes at k-1, k)
     const int km = wrap_dn(k0, dm.nz);
     const int ckm = r0 + km * plane, ck0 = r0 + k0 * plane;
-    T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
     T vz_0 = vtavg(S0, S1, VT, n, ck0, 2, (const T*)nullptr);
-    T s_m[NP], s_0[NP], s_p[NP], dl_m[NP], dl_0[NP];
+    T s_0[NP], s_p[NP], dl_0[NP], fz_m[NP];
     {
+        const T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
         const int ckm2 = r0 + wrap_any(k0 - 2, dm.nz) * plane, ckp = r0 + wrap_up(k0, dm.nz) * plane;
 #pragma unroll
         for (int p = 0; p < NP; ++p)
             if (p < npass) {
                 const T* s = fld(SH, p, n);
-                const T sm2 = s[ckm2];
-                s_m[p] = s[ckm];
+                const T sm2 = s[ckm2], sm = s[ckm];
                 s_0[p] = s[ck0];
                 s_p[p] = s[ckp];
-                dl_m[p] = minmod(sm2, s_m[p], s_0[p]);
-                dl_0[p] = minmod(s_m[p], s_0[p], s_p[p]);
+                const T dlm = minmod(sm2, sm, s_0[p]);
+                dl_0[p] = minmod(sm, s_0[p], s_p[p]);
+                fz_m[p] = upwind_flux(sm + T(0.5) * dlm, s_0[p] - T(0.5) * dl_0[p], T(0.5) * (vz_m + vz_0));
             }
     }
     for (int k = k0; k < k1; ++k) {
@@ -1593,20 +1768,17 @@ __global__ void __launch_bounds__(kBX, (sizeof(T) == 4 && NP <= 4) ? 8 : 1) k_pa
                 dF[1] = Fp - Fm;
             }
             {
-                const T sm = s_m[p], sp = s_p[p], sp2 = s[czp2];
-                const T dlm = dl_m[p], dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
+                const T sp = s_p[p], sp2 = s[czp2];
+                const T dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
                 const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vz_0 + vz_p));
-                const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vz_m + vz_0));
-                dF[2] = Fp - Fm;
-                s_m[p] = s0;
+                dF[2] = Fp - fz_m[p];
+                fz_m[p] = Fp;
                 s_0[p] = sp;
                 s_p[p] = sp2;
-                dl_m[p] = dl0;
                 dl_0[p] = dlp;
             }
             fld(S1, 10 + p, n)[c] = fld(S0, 10 + p, n)[c] - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
         }
-        vz_m = vz_0;
         vz_0 = vz_p;
     }
 }
@@ -1664,14 +1836,41 @@ __global__ void __launch_bounds__(kTmaTile, 8) k_passive_corr_tma(BatchArgs ba) 
     const int nrows = 7 * npass + 5;
     const int ih = (i0 == 0 ? dm.nx : i0) - HE;       // left halo: cells i0-HE .. i0-1
     const int ir = (i0 + kTmaTile) % dm.nx;            // right halo: cells i0+128 .. i0+128+HE-1
+    // each staged row's source at plane 0 and plane offset (the z stencil's
+    // rows lead by one or two planes), worked out once: scalar p: SH rows
+    // j-2..j+2 at 6p..6p+4, step-start row j at 6p+5; then v_x row j, v_y
+    // rows j-1, j, j+1; scalar p at k+2; v_z at k+1.  Rows 6p+2 and the v_x
+    // row carry the 16-byte halo segments.
+    __shared__ const T* row_src[ptma_rows<T, NP>()];
+    __shared__ unsigned char row_dk[ptma_rows<T, NP>()];
     if (t == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init_fence();
     }
+    for (int R = t; R < nrows; R += kTmaTile) {
+        const T* base;
+        int jr = j, dk = 0;
+        if (R < 6 * npass) {
+            const int p = R / 6, q = R % 6;
+            if (q < 5) { base = fld(SH, p, n); jr = wrap_any(j + q - 2, dm.ny); }
+            else base = fld(S0, 10 + p, n);
+        } else if (R < 6 * npass + 4) {
+            const int q = R - 6 * npass;
+            if (q == 0) base = VT;
+            else { base = VT + (size_t)n; jr = wrap_any(j + q - 2, dm.ny); }
+        } else if (R < 7 * npass + 4) {
+            base = fld(SH, R - 6 * npass - 4, n);
+            dk = 2;
+        } else {
+            base = VT + (size_t)6 * n;
+            dk = 1;
+        }
+        row_src[R] = base + i0 + (size_t)dm.nx * jr;
+        row_dk[R] = (unsigned char)dk;
+    }
     __syncthreads();
-    // rows of plane k into stage g: scalar p: SH rows j-2..j+2 at 6p..6p+4,
-    // step-start row j at 6p+5; then v_x row j, v_y rows j-1, j, j+1
+    const int hl = ih - i0, hr = ir - i0;       // halo segments relative to the row segment
     auto issue = [&](int g, int k) {
         T* rows = (T*)(ptma_smem + (size_t)g * ptma_stage_bytes<T, NP>());
         unsigned long long* bar = &bars[g];
@@ -1679,29 +1878,13 @@ __global__ void __launch_bounds__(kTmaTile, 8) k_passive_corr_tma(BatchArgs ba) 
             mbar_expect_tx(bar, (unsigned)(nrows * kTmaTile * (int)sizeof(T) + (2 * npass + 2) * 16));
         __syncwarp();
         for (int R = t; R < nrows; R += 32) {
-            const T* base;
-            int jr = j, kr = k;
-            bool halo = false;
-            if (R < 6 * npass) {
-                const int p = R / 6, q = R % 6;
-                if (q < 5) { base = fld(SH, p, n); jr = wrap_any(j + q - 2, dm.ny); halo = (q == 2); }
-                else base = fld(S0, 10 + p, n);
-            } else if (R < 6 * npass + 4) {
-                const int q = R - 6 * npass;
-                if (q == 0) { base = VT; halo = true; }
-                else { base = VT + (size_t)n; jr = wrap_any(j + q - 2, dm.ny); }
-            } else if (R < 7 * npass + 4) {   // the z stencil's new values: scalar p at k+2, v_z at k+1
-                base = fld(SH, R - 6 * npass - 4, n);
-                kr = wrap_any(k + 2, dm.nz);
-            } else {
-                base = VT + (size_t)6 * n;
-                kr = wrap_up(k, dm.nz);
-            }
-            const size_t ofs = (size_t)dm.nx * (jr + (size_t)dm.ny * kr);
-            bulk_g2s(rows + R * RS + HE, base + i0 + ofs, kTmaTile * (unsigned)sizeof(T), bar);
-            if (halo) {
-                bulk_g2s(rows + R * RS, base + ih + ofs, 16u, bar);
-                bulk_g2s(rows + R * RS + HE + kTmaTile, base + ir + ofs, 16u, bar);
+            int kr = k + row_dk[R];
+            while (kr >= dm.nz) kr -= dm.nz;
+            const T* src = row_src[R] + (size_t)plane * kr;
+            bulk_g2s(rows + R * RS + HE, src, kTmaTile * (unsigned)sizeof(T), bar);
+            if ((R < 6 * npass && R % 6 == 2) || R == 6 * npass) {
+                bulk_g2s(rows + R * RS, src + hl, 16u, bar);
+                bulk_g2s(rows + R * RS + HE + kTmaTile, src + hr, 16u, bar);
             }
         }
     };
@@ -1718,25 +1901,25 @@ __global__ void __launch_bounds__(kTmaTile, 8) k_passive_corr_tma(BatchArgs ba) 
     const T* up_z = drive ? mbnd + (size_t)4 * plane_stride + r0 : nullptr;
     const int rxm = wrap_dn(i, dm.nx) + dm.nx * j, rxp = wrap_up(i, dm.nx) + dm.nx * j;
     const int rym = i + dm.nx * wrap_dn(j, dm.ny), ryp = i + dm.nx * wrap_up(j, dm.ny);
-    // z window of the column: v_z at k-1, k; scalars at k-1..k+1 and the
-    // minmod slopes at k-1, k
+    // z window of the column: v_z at k; scalars at k, k+1, the minmod slope
+    // at k and the flux through the face k-1/2
     const int km = wrap_dn(k0, dm.nz);
     const int ckm = r0 + km * plane, ck0 = r0 + k0 * plane;
-    T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
     T vz_0 = vtavg(S0, S1, VT, n, ck0, 2, (const T*)nullptr);
-    T s_m[NP], s_0[NP], s_p[NP], dl_m[NP], dl_0[NP];
+    T s_0[NP], s_p[NP], dl_0[NP], fz_m[NP];
     {
+        const T vz_m = vtavg(S0, S1, VT, n, ckm, 2, (k0 == 0) ? um_z : (const T*)nullptr);
         const int ckm2 = r0 + wrap_any(k0 - 2, dm.nz) * plane, ckp = r0 + wrap_up(k0, dm.nz) * plane;
 #pragma unroll
         for (int p = 0; p < NP; ++p)
             if (p < npass) {
                 const T* s = fld(SH, p, n);
-                const T sm2 = s[ckm2];
-                s_m[p] = s[ckm];
+                const T sm2 = s[ckm2], sm = s[ckm];
                 s_0[p] = s[ck0];
                 s_p[p] = s[ckp];
-                dl_m[p] = minmod(sm2, s_m[p], s_0[p]);
-                dl_0[p] = minmod(s_m[p], s_0[p], s_p[p]);
+                const T dlm = minmod(sm2, sm, s_0[p]);
+                dl_0[p] = minmod(sm, s_0[p], s_p[p]);
+                fz_m[p] = upwind_flux(sm + T(0.5) * dlm, s_0[p] - T(0.5) * dl_0[p], T(0.5) * (vz_m + vz_0));
             }
     }
     bool ok = true;
@@ -1780,20 +1963,17 @@ __global__ void __launch_bounds__(kTmaTile, 8) k_passive_corr_tma(BatchArgs ba) 
                     dF[1] = Fp - Fm;
                 }
                 {
-                    const T sm = s_m[p], sp = s_p[p], sp2 = at(6 * npass + 4 + p, 0);
-                    const T dlm = dl_m[p], dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
+                    const T sp = s_p[p], sp2 = at(6 * npass + 4 + p, 0);
+                    const T dl0 = dl_0[p], dlp = minmod(s0, sp, sp2);
                     const T Fp = upwind_flux(s0 + T(0.5) * dl0, sp - T(0.5) * dlp, T(0.5) * (vz_0 + vz_p));
-                    const T Fm = upwind_flux(sm + T(0.5) * dlm, s0 - T(0.5) * dl0, T(0.5) * (vz_m + vz_0));
-                    dF[2] = Fp - Fm;
-                    s_m[p] = s0;
+                    dF[2] = Fp - fz_m[p];
+                    fz_m[p] = Fp;
                     s_0[p] = sp;
                     s_p[p] = sp2;
-                    dl_m[p] = dl0;
                     dl_0[p] = dlp;
                 }
                 fld(S1, 10 + p, n)[c] = at(6 * p + 5, 0) - dtdx * (vx0 * dF[0] + vy0 * dF[1] + vz_0 * dF[2]);
             }
-            vz_m = vz_0;
             vz_0 = vz_p;
         }
         __syncthreads();   // every thread is done with stage g before it is refilled

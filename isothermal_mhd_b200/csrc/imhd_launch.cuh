@@ -61,6 +61,25 @@ static dim3 grid_of(const BatchDev& b, int kind) {
     }
 }
 
+// Corner EMFs of one stage (PROT: of the protection fluxes): single boxes
+// whose rows are whole 32-cell segments and whose y edge is a multiple of 8
+// take the tiled kernel with shared cell-centre values, the rest the
+// z-column kernel.
+template <class T, bool ONE, bool PROT>
+static void launch_emf(BatchDev& b, dim3 gz, int half_step_state) {
+    if constexpr (ONE) {
+        const BoxRec& r = b.a.one;
+        if (emf_by_tiles(r.nx, r.ny)) {
+            dim3 g((unsigned)(r.nx / kEmfTX), (unsigned)(r.ny / kEmfTY), (unsigned)((r.nz + kEmfSegZ - 1) / kEmfSegZ));
+            k_corner_emf_tile<T, PROT><<<g, kEmfThreads, 0, b.st>>>(b.a, half_step_state);
+            b.launches += 1;
+            return;
+        }
+    }
+    k_corner_emf<T, ONE, PROT><<<gz, kBX, 0, b.st>>>(b.a, half_step_state);
+    b.launches += 1;
+}
+
 template <class T, int SCHEME, bool ONE>
 static void launch_fluxes_pred(BatchDev& b) {
     if (!b.has_scheme[SCHEME] || b.totals[scheme_kind(SCHEME, kSubCell)] == 0) return;
@@ -205,7 +224,7 @@ static void launch_fluxes_corr_x(BatchDev& b) {
         dim3 gr = grid_of<ONE>(b, scheme_kind(SCHEME, kSubXRow));
         size_t smem = 13 * (size_t)b.row_nx_max * sizeof(T);
         ensure_xrow_attr<T, SCHEME, ONE>();
-        int bd = b.row_nx_max >= 256 ? 256 : ((b.row_nx_max + 31) / 32) * 32;
+        int bd = b.row_nx_max >= 128 ? 128 : ((b.row_nx_max + 31) / 32) * 32;
         k_corr_flux_xrow<T, SCHEME, ONE><<<gr, bd, smem, b.st>>>(b.a);
         b.launches += 1;
     }
@@ -265,12 +284,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStPredFlux);
     for_schemes([&](auto s) { launch_fluxes_pred<T, s.value, ONE>(b); });
     mark(b, kStPredEmf);
-    k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 0);
-    b.launches += 1;
-    if (b.any_protect) {
-        k_corner_emf<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 0);
-        b.launches += 1;
-    }
+    launch_emf<T, ONE, false>(b, gz, 0);
+    if (b.any_protect) launch_emf<T, ONE, true>(b, gz, 0);
     mark(b, kStPredUpdate);
     launch_update<T, ONE>(b, 0.5, 0);   // counts its own launches
     if (b.any_protect) launch_protection<T, ONE>(b, 0.5, 0);
@@ -283,12 +298,8 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     mark(b, kStCorrFluxZ);
     for_schemes([&](auto s) { launch_fluxes_corr_march<T, s.value, 2, ONE>(b); });
     mark(b, kStCorrEmf);
-    k_corner_emf<T, ONE><<<gz, kBX, 0, b.st>>>(b.a, 1);
-    b.launches += 1;
-    if (b.any_protect) {
-        k_corner_emf<T, ONE, true><<<gz, kBX, 0, b.st>>>(b.a, 1);
-        b.launches += 1;
-    }
+    launch_emf<T, ONE, false>(b, gz, 1);
+    if (b.any_protect) launch_emf<T, ONE, true>(b, gz, 1);
     mark(b, kStFinalUpdate);
     launch_update<T, ONE>(b, 1.0, 1);
     if (b.any_protect) launch_protection<T, ONE>(b, 1.0, 1);

@@ -4,14 +4,16 @@
 // Requests (a box configuration, a step count, an initial condition given as
 // a uniform state plus Fourier velocity modes, and optional forcing modes)
 // arrive through imhd_server_submit from any host thread.  One worker thread
-// owns the device: it admits queued requests in arrival order while their
-// device bytes fit the HBM budget, builds each admitted box on the device
-// (uniform state, Fourier velocity, force field, clock), and advances all
-// resident boxes together with the batched step (one launch per stage over a
-// table of every resident box, per-box device clocks, the step captured as a
-// CUDA graph).  Every few replays it reads all clocks in one copy, retires
-// the boxes that finished (download to host, free their memory) and admits
-// new ones, so requests that arrive while others run join the running batch.
+// steps the resident boxes: all of them together with the batched step (one
+// launch per stage over a table of every resident box, per-box device
+// clocks, the step captured as a CUDA graph).  A builder thread admits queued
+// requests in arrival order while their device bytes fit the HBM budget and
+// builds each one (uniform state, Fourier velocity, force field, clock) on a
+// stream of its own while the worker steps; built boxes join the resident
+// set at the worker's next round.  Every few replays the worker reads all
+// clocks in one copy and retires the boxes that finished to a harvester
+// thread (download to host, free their memory), so requests that arrive
+// while others run join the running batch.
 //
 // A box computes the same bits whatever else is resident: every launch runs
 // the same kernels on each box's own data, and no box reads another's.
@@ -72,6 +74,7 @@ struct Resident {
     size_t bytes = 0;
     int cur = 0;               // buffer holding the current state
     double t_admit = 0;
+    cudaEvent_t ev = nullptr;  // end of the box's build on the builder's stream
 };
 
 struct Result {
@@ -104,6 +107,10 @@ struct imhd_server {
     long long resident = 0, peak_resident = 0;
     long long resident_cells_ = 0;
     double t_build = 0, t_rebuild = 0, t_step = 0, t_retire = 0, t_harvest = 0;   // seconds per phase
+    // built boxes waiting to join the resident set (builder thread -> worker)
+    std::deque<Resident> ready;
+    int building = 0;                        // boxes the builder is building right now
+    bool worker_exit = false;                // the worker left its loop (the builder stops too)
     // finished boxes waiting for their download (harvester thread)
     std::deque<Resident> harvest_q;
     std::condition_variable cv_h;
@@ -146,9 +153,12 @@ struct Worker {
     double* clocks_dev = nullptr;
     double* clocks_host = nullptr;   // pinned
     size_t clocks_cap = 0;
+    // builder thread state (its stream, mode buffers and error)
+    cudaStream_t bst = nullptr;
     int* modes_dev = nullptr;
     double* amps_dev = nullptr;
     size_t modes_cap = 0;
+    std::string berr;
     std::string err;
 
     explicit Worker(imhd_server* srv) : s(srv), f64(srv->cfg.precision == 64) { b.precision = srv->cfg.precision; }
@@ -178,6 +188,15 @@ struct Worker {
         if (clocks_host) cudaFreeHost(clocks_host);
         if (st) cudaStreamDestroy(st);
         st = nullptr;
+        if (bst) cudaStreamDestroy(bst);
+        bst = nullptr;
+    }
+
+    // ---- builder thread: builds admitted boxes on a stream of its own
+    bool bck(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return true;
+        if (berr.empty()) berr = std::string(what) + ": " + cudaGetErrorString(e);
+        return false;
     }
 
     bool ensure_modes(size_t m) {
@@ -187,22 +206,22 @@ struct Worker {
         modes_dev = nullptr;
         amps_dev = nullptr;
         modes_cap = 0;
-        if (!ck(cudaMalloc((void**)&modes_dev, m * 3 * sizeof(int)), "mode allocation")) return false;
-        if (!ck(cudaMalloc((void**)&amps_dev, m * 6 * sizeof(double)), "mode allocation")) return false;
+        if (!bck(cudaMalloc((void**)&modes_dev, m * 3 * sizeof(int)), "mode allocation")) return false;
+        if (!bck(cudaMalloc((void**)&amps_dev, m * 6 * sizeof(double)), "mode allocation")) return false;
         modes_cap = m;
         return true;
     }
 
-    // Build an admitted request on the device: buffers, uniform state,
-    // Fourier velocity, force field, clock.  False: out of device memory
-    // (nothing kept) or a CUDA error (err set).
+    // Build an admitted request on the device, on the builder's stream:
+    // buffers, uniform state, Fourier velocity, force field, clock.  False:
+    // out of device memory (nothing kept) or a CUDA error (berr set).
     bool build(Resident& r) {
         const Request& q = r.req;
         const imhd_config& c = q.cfg;
         imhd::init_rec(r.rec, c.nx, c.ny, c.nz, c.npass, c.riemann, c.recon, c.sound_speed, c.cour, c.edot, c.dt_turb,
                        c.protect);
         r.bytes = imhd::box_bytes(r.rec, s->esz, q.forcing != 0);
-        cudaError_t e = cudaMallocAsync(&r.mem, r.bytes, st);
+        cudaError_t e = cudaMallocAsync(&r.mem, r.bytes, bst);
         if (e != cudaSuccess) {
             cudaGetLastError();
             r.mem = nullptr;
@@ -210,28 +229,28 @@ struct Worker {
         }
         imhd::carve_box(r.rec, (unsigned char*)r.mem, s->esz, q.forcing != 0);
         r.cur = 0;
-        if (!ck(cudaMemsetAsync(r.mem, 0, r.bytes, st), "box clear")) return false;
-        if (!ck(f64 ? imhd::run_init_uniform<double>(st, r.rec, 0, q.rho, q.b0)
-                    : imhd::run_init_uniform<float>(st, r.rec, 0, q.rho, q.b0), "uniform state")) return false;
+        if (!bck(cudaMemsetAsync(r.mem, 0, r.bytes, bst), "box clear")) return false;
+        if (!bck(f64 ? imhd::run_init_uniform<double>(bst, r.rec, 0, q.rho, q.b0)
+                    : imhd::run_init_uniform<float>(bst, r.rec, 0, q.rho, q.b0), "uniform state")) return false;
         size_t m = q.kvec.size() / 3;
         if (m) {
             if (!ensure_modes(m)) return false;
-            if (!ck(cudaMemcpyAsync(modes_dev, q.kvec.data(), m * 3 * sizeof(int), cudaMemcpyHostToDevice, st), "modes"))
+            if (!bck(cudaMemcpyAsync(modes_dev, q.kvec.data(), m * 3 * sizeof(int), cudaMemcpyHostToDevice, bst), "modes"))
                 return false;
             if (!q.amp_v.empty()) {
-                if (!ck(cudaMemcpyAsync(amps_dev, q.amp_v.data(), m * 6 * sizeof(double), cudaMemcpyHostToDevice, st),
+                if (!bck(cudaMemcpyAsync(amps_dev, q.amp_v.data(), m * 6 * sizeof(double), cudaMemcpyHostToDevice, bst),
                         "velocity modes")) return false;
-                if (!ck(f64 ? imhd::run_ou_field<double>(st, r.rec, 0, 0, modes_dev, amps_dev, (int)m, q.scale_v)
-                            : imhd::run_ou_field<float>(st, r.rec, 0, 0, modes_dev, amps_dev, (int)m, q.scale_v),
+                if (!bck(f64 ? imhd::run_ou_field<double>(bst, r.rec, 0, 0, modes_dev, amps_dev, (int)m, q.scale_v)
+                            : imhd::run_ou_field<float>(bst, r.rec, 0, 0, modes_dev, amps_dev, (int)m, q.scale_v),
                         "velocity field")) return false;
             }
             if (q.forcing) {
                 // the velocity launch must finish reading amps_dev first
-                if (!ck(cudaStreamSynchronize(st), "velocity field")) return false;
-                if (!ck(cudaMemcpyAsync(amps_dev, q.amp_f.data(), m * 6 * sizeof(double), cudaMemcpyHostToDevice, st),
+                if (!bck(cudaStreamSynchronize(bst), "velocity field")) return false;
+                if (!bck(cudaMemcpyAsync(amps_dev, q.amp_f.data(), m * 6 * sizeof(double), cudaMemcpyHostToDevice, bst),
                         "force modes")) return false;
-                if (!ck(f64 ? imhd::run_ou_field<double>(st, r.rec, 0, 1, modes_dev, amps_dev, (int)m, q.scale_f)
-                            : imhd::run_ou_field<float>(st, r.rec, 0, 1, modes_dev, amps_dev, (int)m, q.scale_f),
+                if (!bck(f64 ? imhd::run_ou_field<double>(bst, r.rec, 0, 1, modes_dev, amps_dev, (int)m, q.scale_f)
+                            : imhd::run_ou_field<float>(bst, r.rec, 0, 1, modes_dev, amps_dev, (int)m, q.scale_f),
                         "force field")) return false;
             }
         }
@@ -240,18 +259,19 @@ struct Worker {
         double dt0 = q.dt0;
         if (!(dt0 > 0.0)) {
             // COUR*dx/cmax of the initial state (get_max_speed_vanleer without smax)
-            if (!ck(cudaMemcpyAsync(r.rec.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, st), "clock")) return false;
-            imhd::BatchDev d = b;
+            if (!bck(cudaMemcpyAsync(r.rec.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, bst), "clock")) return false;
+            imhd::BatchDev d;
+            d.precision = s->cfg.precision;
             d.a.use_one = 1;
             d.a.one = r.rec;
             d.a.one.active = 1;
             d.a.nbox = 1;
             for (int k = 0; k < imhd::kKinds; ++k) d.totals[k] = (int)imhd::blocks_of(r.rec, k, s->esz);
-            d.st = st;
-            if (!ck(f64 ? imhd::run_max_speed<double>(d) : imhd::run_max_speed<float>(d), "initial CFL")) return false;
+            d.st = bst;
+            if (!bck(f64 ? imhd::run_max_speed<double>(d) : imhd::run_max_speed<float>(d), "initial CFL")) return false;
             imhd::Scalars back;
-            if (!ck(cudaMemcpyAsync(&back, r.rec.sc, sizeof(back), cudaMemcpyDeviceToHost, st), "initial CFL")) return false;
-            if (!ck(cudaStreamSynchronize(st), "initial CFL")) return false;
+            if (!bck(cudaMemcpyAsync(&back, r.rec.sc, sizeof(back), cudaMemcpyDeviceToHost, bst), "initial CFL")) return false;
+            if (!bck(cudaStreamSynchronize(bst), "initial CFL")) return false;
             double mx = 0.0;
             for (int k = 0; k < imhd::kSlots; ++k) {
                 double v;
@@ -268,9 +288,9 @@ struct Worker {
         sc.steps_target = q.steps;
         sc.forcing = q.forcing;
         sc.active = (q.steps > 0 && 0.0 < q.t_end) ? 1 : 0;
-        if (!ck(cudaMemcpyAsync(r.rec.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, st), "clock")) return false;
+        if (!bck(cudaMemcpyAsync(r.rec.sc, &sc, sizeof(sc), cudaMemcpyHostToDevice, bst), "clock")) return false;
         r.rec.active = sc.active;
-        return ck(cudaStreamSynchronize(st), "box build");
+        return bck(cudaStreamSynchronize(bst), "box build");
     }
 
     // Table of the resident boxes (current state first) and the step graph.
@@ -329,71 +349,141 @@ struct Worker {
         return true;
     }
 
-    // Admit queued requests in arrival order while they fit.
-    bool admit() {
+    // Builder thread: admit queued requests in arrival order while their
+    // bytes fit the budget (and the resident cells the cell limit) and build
+    // them on the builder's own stream, overlapping the worker's steps; a
+    // built box waits in `ready` with an event the worker's stream waits on.
+    void build_loop() {
+        cudaSetDevice(s->cfg.device);
+        const bool stream_ok = cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking) == cudaSuccess;
+        // after an allocation failure: admit again only once the reserved
+        // bytes fell below this mark (a retirement freed memory)
+        size_t retry_below = 0;
         for (;;) {
             Request q;
+            size_t need = 0;
+            long long cells = 0;
             {
-                std::lock_guard<std::mutex> lk(s->mu);
-                if (s->queue.empty()) return true;
-                const Request& h = s->queue.front();
-                imhd::BoxRec probe;
-                imhd::init_rec(probe, h.cfg.nx, h.cfg.ny, h.cfg.nz, h.cfg.npass, h.cfg.riemann, h.cfg.recon, h.cfg.sound_speed,
-                               h.cfg.cour, h.cfg.edot, h.cfg.dt_turb, h.cfg.protect);
-                size_t need = imhd::box_bytes(probe, s->esz, h.forcing != 0);
-                long long cells = (long long)h.cfg.nx * h.cfg.ny * h.cfg.nz;
-                bool over_budget = (double)(s->used_bytes + need) > s->cfg.hbm_budget_bytes;
-                bool over_cells = s->cfg.max_resident_cells > 0 && !live.empty() &&
-                                  (s->resident_cells_ + cells) > s->cfg.max_resident_cells;
-                if (over_budget || over_cells) {
-                    if (live.empty() && (double)need > s->cfg.hbm_budget_bytes) {
-                        Result& res = s->results[h.id];
-                        res.state = IMHD_REQ_FAILED;
-                        res.error = "request needs more device memory than the whole budget";
-                        res.t_done = now_s();
-                        s->failed += 1;
-                        s->queue.pop_front();
-                        continue;
+                std::unique_lock<std::mutex> lk(s->mu);
+                bool got = false;
+                while (!got) {
+                    if (s->worker_exit || (s->stopping && (!s->drain || s->queue.empty()))) {
+                        if (bst) cudaStreamSynchronize(bst);
+                        return;
                     }
-                    return true;
+                    if (!stream_ok) {
+                        if (s->fatal.empty()) s->fatal = "builder stream creation failed";
+                        s->cv.notify_all();
+                        return;
+                    }
+                    if (retry_below && s->used_bytes < retry_below) retry_below = 0;
+                    if (!s->queue.empty() && !retry_below) {
+                        const Request& h = s->queue.front();
+                        imhd::BoxRec probe;
+                        imhd::init_rec(probe, h.cfg.nx, h.cfg.ny, h.cfg.nz, h.cfg.npass, h.cfg.riemann, h.cfg.recon,
+                                       h.cfg.sound_speed, h.cfg.cour, h.cfg.edot, h.cfg.dt_turb, h.cfg.protect);
+                        need = imhd::box_bytes(probe, s->esz, h.forcing != 0);
+                        cells = (long long)h.cfg.nx * h.cfg.ny * h.cfg.nz;
+                        // nothing resident, built or downloading: the request is alone
+                        const bool alone = s->used_bytes == 0;
+                        const bool over_budget = (double)(s->used_bytes + need) > s->cfg.hbm_budget_bytes;
+                        const bool over_cells = s->cfg.max_resident_cells > 0 && !alone &&
+                                                (s->resident_cells_ + cells) > s->cfg.max_resident_cells;
+                        if (!(over_budget || over_cells)) {
+                            q = std::move(s->queue.front());
+                            s->queue.pop_front();
+                            s->used_bytes += need;          // reserved until the harvester frees the box
+                            s->resident_cells_ += cells;
+                            s->building += 1;
+                            got = true;
+                            break;
+                        }
+                        if (alone && (double)need > s->cfg.hbm_budget_bytes) {
+                            Result& res = s->results[h.id];
+                            res.state = IMHD_REQ_FAILED;
+                            res.error = "request needs more device memory than the whole budget";
+                            res.t_done = now_s();
+                            s->failed += 1;
+                            s->queue.pop_front();
+                            continue;
+                        }
+                    }
+                    // wait for a request, or for a retirement to free memory
+                    s->cv.wait_for(lk, std::chrono::milliseconds(20));
                 }
-                q = std::move(s->queue.front());
-                s->queue.pop_front();
             }
             Resident r;
             r.req = std::move(q);
             r.t_admit = now_s();
+            const double t0 = now_s();
             bool ok = build(r);
-            if (!ok && !err.empty()) {
-                if (r.mem) cudaFree(r.mem);
-                return false;
-            }
+            if (ok) ok = bck(cudaEventCreateWithFlags(&r.ev, cudaEventDisableTiming), "build event") &&
+                         bck(cudaEventRecord(r.ev, bst), "build event");
             std::lock_guard<std::mutex> lk(s->mu);
+            s->building -= 1;
+            s->t_build += now_s() - t0;
             if (!ok) {
-                // device memory is short: put it back and wait for a retirement
-                if (live.empty()) {
+                s->used_bytes -= need;
+                s->resident_cells_ -= cells;
+                if (r.mem) cudaFreeAsync(r.mem, bst);
+                if (r.ev) cudaEventDestroy(r.ev);
+                if (!berr.empty()) {       // CUDA error: the server stops
+                    if (s->fatal.empty()) s->fatal = berr;
+                    Result& res = s->results[r.req.id];
+                    res.state = IMHD_REQ_FAILED;
+                    res.error = berr;
+                    res.t_done = now_s();
+                    s->failed += 1;
+                    s->cv.notify_all();
+                    return;
+                }
+                // device memory is short: back to the queue until a retirement,
+                // or failed when nothing else holds memory
+                if (s->used_bytes == 0) {
                     Result& res = s->results[r.req.id];
                     res.state = IMHD_REQ_FAILED;
                     res.error = "device allocation failed";
                     res.t_done = now_s();
                     s->failed += 1;
-                    continue;
+                } else {
+                    s->queue.push_front(std::move(r.req));
+                    retry_below = s->used_bytes;
                 }
-                s->queue.push_front(std::move(r.req));
-                return true;
+                continue;
             }
             Result& res = s->results[r.req.id];
             res.state = IMHD_REQ_RUNNING;
             res.t_admit = r.t_admit;
             s->admitted += 1;
-            s->used_bytes += r.bytes;
             s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
-            s->resident_cells_ += (long long)r.rec.n;
-            live.push_back(std::move(r));
-            s->resident = (long long)live.size();
-            s->peak_resident = std::max(s->peak_resident, s->resident);
-            dirty = true;
+            s->ready.push_back(std::move(r));
+            s->cv.notify_all();
         }
+    }
+
+    // Worker: the built boxes join the resident set (the worker's stream
+    // waits for their builds).  False on a CUDA error.
+    bool take_ready() {
+        std::deque<Resident> got;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            got.swap(s->ready);
+        }
+        if (got.empty()) return true;
+        bool ok = true;
+        for (Resident& r : got) {
+            if (r.ev) {
+                ok = ok && ck(cudaStreamWaitEvent(st, r.ev, 0), "build wait");
+                cudaEventDestroy(r.ev);
+                r.ev = nullptr;
+            }
+            live.push_back(std::move(r));
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->resident = (long long)live.size();
+        s->peak_resident = std::max(s->peak_resident, s->resident);
+        dirty = true;
+        return ok;
     }
 
     // Read every clock; retire the boxes that stopped.
@@ -456,24 +546,21 @@ struct Worker {
         }
         const int per_round = s->cfg.steps_per_round > 0 ? s->cfg.steps_per_round : 4;
         std::thread harvester([this]() { harvest_loop(); });
+        std::thread builder([this]() { build_loop(); });
         for (;;) {
             {
                 std::unique_lock<std::mutex> lk(s->mu);
-                if (s->stopping && (!s->drain || (s->queue.empty() && live.empty()))) break;
-                if (live.empty() && s->queue.empty()) {
-                    s->cv.wait_for(lk, std::chrono::milliseconds(50));
+                if (!s->fatal.empty()) break;        // the builder stopped on a CUDA error
+                const bool idle = live.empty() && s->ready.empty();
+                if (s->stopping && (!s->drain || (s->queue.empty() && idle && s->building == 0))) break;
+                if (idle) {
+                    s->cv.wait_for(lk, std::chrono::milliseconds(5));
                     continue;
                 }
             }
-            double t0 = now_s();
-            if (!admit()) break;
             double t1 = now_s();
-            if (live.empty()) {
-                std::unique_lock<std::mutex> lk(s->mu);
-                s->t_build += t1 - t0;
-                s->cv.wait_for(lk, std::chrono::milliseconds(5));
-                continue;
-            }
+            if (!take_ready()) break;
+            if (live.empty()) continue;
             if (dirty && !rebuild()) break;
             double t2 = now_s();
             bool ok = true;
@@ -486,11 +573,18 @@ struct Worker {
             std::lock_guard<std::mutex> lk(s->mu);
             s->replays += per_round;
             s->launches += per_round * graph_kernels;
-            s->t_build += t1 - t0;
             s->t_rebuild += t2 - t1;
             s->t_step += t3 - t2;
             s->t_retire += t4 - t3;
         }
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->worker_exit = true;
+            s->cv.notify_all();
+        }
+        builder.join();
+        // boxes built but never stepped (stop without drain, or an error)
+        take_ready();
         {
             std::lock_guard<std::mutex> lk(s->mu);
             s->harvest_stop = true;
@@ -533,6 +627,7 @@ struct Worker {
             std::lock_guard<std::mutex> lk(s->mu);
             s->used_bytes -= r.bytes;
             s->t_harvest += now_s() - t0;
+            s->cv.notify_all();           // the builder may admit now
             if (r.req.steps < 0) continue;               // failed: result already recorded
             Result& res = s->results[r.req.id];
             if (e != cudaSuccess || !hs) {
