@@ -778,167 +778,6 @@ __global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(Batc
     }
 }
 
-// ------------------------------------------- corner EMF, shared cell-centre values
-// The corner EMFs of a single box whose rows are whole 32-cell segments and
-// whose y edge is a multiple of 8: a block owns a 32 x 8 tile of columns and
-// walks kEmfSegZ planes.  Each plane's cell-centre EMFs and velocities are
-// computed once per cell into a three-plane ring in shared memory (a ninth
-// warp computes the tile's +y row and +x column), and the corners read their
-// neighbours' values from there; the z-column kernel above computes each
-// cell's values three times and one component a fourth.  The same operations
-// on the same operands: the results are those of k_corner_emf.  One barrier
-// per plane: plane k+1 goes to the slot of plane k-2, which every thread
-// finished reading before it arrived at the barrier of plane k-1.
-constexpr int kEmfTX = 32, kEmfTY = 8, kEmfSegZ = 32;
-constexpr int kEmfThreads = kEmfTX * (kEmfTY + 1);
-__host__ __device__ __forceinline__ bool emf_by_tiles(int nx, int ny) {
-    return nx % kEmfTX == 0 && ny % kEmfTY == 0;
-}
-
-template <class T>
-struct EmfRing {                       // [slot][ux, uy, ex, ey, ez][row][column]
-    T v[3][5][kEmfTY + 1][kEmfTX + 1];
-};
-template <class T>
-__device__ __forceinline__ void ring_put(EmfRing<T>& R, int s, int y, int x, const CellEV<T>& a) {
-    R.v[s][0][y][x] = a.ux;
-    R.v[s][1][y][x] = a.uy;
-    R.v[s][2][y][x] = a.ex;
-    R.v[s][3][y][x] = a.ey;
-    R.v[s][4][y][x] = a.ez;
-}
-
-template <class T, bool PROT = false>
-__global__ void __launch_bounds__(kEmfThreads, sizeof(T) == 4 ? 3 : 1) k_corner_emf_tile(BatchArgs ba,
-                                                                                           int half_step_state) {
-    __shared__ EmfRing<T> ring;
-    const BoxRec rp = ba.one;
-    if (!rp.active || (PROT && !rp.protect)) return;
-    const Dims dm = dims_of(rp);
-    const T* __restrict__ S = (const T*)(half_step_state ? rp.S[1] : rp.S[0]);
-    const T* __restrict__ F = (const T*)(PROT ? rp.Fp : rp.F);
-    T* __restrict__ E = (T*)(PROT ? rp.Ep : rp.E);
-    const int lx = (int)threadIdx.x & 31, ly = (int)threadIdx.x >> 5;   // ly == kEmfTY: the halo warp
-    const int i0 = (int)blockIdx.x * kEmfTX, j0 = (int)blockIdx.y * kEmfTY;
-    const int k0 = (int)blockIdx.z * kEmfSegZ, k1 = min(k0 + kEmfSegZ, dm.nz);
-    const int n = dm.n, plane = dm.nx * dm.ny;
-    const bool out = ly < kEmfTY;
-    // the cells whose values this thread computes per plane: its own column
-    // (a halo-warp lane: row j0+8) and, lanes 0..8 of the halo warp, rows
-    // j0..j0+8 of column i0+32 (periodic images at the box edges)
-    const int jh = (j0 + kEmfTY == dm.ny) ? 0 : j0 + kEmfTY;
-    const int ih = (i0 + kEmfTX == dm.nx) ? 0 : i0 + kEmfTX;
-    const int ra = i0 + lx + dm.nx * (out ? j0 + ly : jh);
-    const bool second = !out && lx <= kEmfTY;
-    const int rb = ih + dm.nx * (lx == kEmfTY ? jh : j0 + lx);
-    const int ya = out ? ly : kEmfTY;
-    // corner neighbours of an output column
-    const int i = i0 + lx, j = j0 + (out ? ly : 0);
-    const int ip = wrap_up(i, dm.nx), jp = wrap_up(j, dm.ny);
-    const int r000 = i + dm.nx * j, r100 = ip + dm.nx * j, r010 = i + dm.nx * jp;
-    const T* Fx_bt1 = F + (size_t)4 * n;
-    const T* Fx_bt2 = F + (size_t)5 * n;
-    const T* Fy_bt1 = F + (size_t)10 * n;
-    const T* Fy_bt2 = F + (size_t)11 * n;
-    const T* Fz_bt1 = F + (size_t)16 * n;
-    const T* Fz_bt2 = F + (size_t)17 * n;
-    int s0 = 0;
-    CellEV<T> own = cell_ev(S, n, ra + k0 * plane);
-    ring_put(ring, s0, ya, lx, own);
-    if (second) ring_put(ring, s0, lx, kEmfTX, cell_ev(S, n, rb + k0 * plane));
-    T fx2_000 = T(0), fy1_000 = T(0);
-    if (out) {
-        fx2_000 = Fx_bt2[r000 + k0 * plane];
-        fy1_000 = Fy_bt1[r000 + k0 * plane];
-    }
-    for (int k = k0; k < k1; ++k) {
-        const int kp = wrap_up(k, dm.nz);
-        const int s1 = (s0 == 2) ? 0 : s0 + 1;
-        const CellEV<T> nxt = cell_ev(S, n, ra + kp * plane);
-        ring_put(ring, s1, ya, lx, nxt);
-        if (second) ring_put(ring, s1, lx, kEmfTX, cell_ev(S, n, rb + kp * plane));
-        __syncthreads();
-        if (out) {
-            const int c000 = r000 + k * plane, c100 = r100 + k * plane, c010 = r010 + k * plane;
-            const int c001 = r000 + kp * plane;
-            const auto& A = ring.v[s0];
-            const auto& B = ring.v[s1];
-            const T x_ux = A[0][ly][lx + 1], x_ey = A[3][ly][lx + 1], x_ez = A[4][ly][lx + 1];
-            const T y_uy = A[1][ly + 1][lx], y_ex = A[2][ly + 1][lx], y_ez = A[4][ly + 1][lx];
-            const T xy_ez = A[4][ly + 1][lx + 1];
-            const T xp_ey = B[3][ly][lx + 1], yp_ex = B[2][ly + 1][lx];
-            const T fx2_001 = Fx_bt2[c001], fy1_001 = Fy_bt1[c001];
-            const T vx = T(0.5) * (own.ux + x_ux);
-            const T vy = T(0.5) * (own.uy + y_uy);
-            const T vz = T(0.5) * (own.uz + nxt.uz);
-            // Ez at (i+1/2, j+1/2, k)
-            {
-                T E31_000 = -Fx_bt1[c000], E31_010 = -Fx_bt1[c010];
-                T E32_000 = Fy_bt2[c000], E32_100 = Fy_bt2[c100];
-                T E33_000 = own.ez, E33_100 = x_ez, E33_010 = y_ez, E33_110 = xy_ez;
-                T dyL14 = T(2) * (E32_000 - E33_000);
-                T dyR14 = T(2) * (E32_100 - E33_100);
-                T dyL34 = T(2) * (E33_010 - E32_000);
-                T dyR34 = T(2) * (E33_110 - E32_100);
-                T dy1214, dy1234;
-                upwind_pair(vx, dyL14, dyR14, dyL34, dyR34, dy1214, dy1234);
-                T dxL14 = T(2) * (E31_000 - E33_000);
-                T dxR14 = T(2) * (E31_010 - E33_010);
-                T dxL34 = T(2) * (E33_100 - E31_000);
-                T dxR34 = T(2) * (E33_110 - E31_010);
-                T dx1412, dx3412;
-                upwind_pair(vy, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
-                E[(size_t)2 * n + c000] = T(0.25) * (E31_000 + E31_010 + E32_000 + E32_100) +
-                                          T(0.125) * ((dy1214 - dy1234) + (dx1412 - dx3412));
-            }
-            // Ey at (i+1/2, j, k+1/2)
-            {
-                T E21_000 = fx2_000, E21_001 = fx2_001;
-                T E22_000 = -Fz_bt1[c000], E22_100 = -Fz_bt1[c100];
-                T E23_000 = own.ey, E23_100 = x_ey, E23_001 = nxt.ey, E23_101 = xp_ey;
-                T dzL14 = T(2) * (E22_000 - E23_000);
-                T dzR14 = T(2) * (E22_100 - E23_100);
-                T dzL34 = T(2) * (E23_001 - E22_000);
-                T dzR34 = T(2) * (E23_101 - E22_100);
-                T dz1214, dz1234;
-                upwind_pair(vx, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
-                T dxL14 = T(2) * (E21_000 - E23_000);
-                T dxR14 = T(2) * (E21_001 - E23_001);
-                T dxL34 = T(2) * (E23_100 - E21_000);
-                T dxR34 = T(2) * (E23_101 - E21_001);
-                T dx1412, dx3412;
-                upwind_pair(vz, dxL14, dxR14, dxL34, dxR34, dx1412, dx3412);
-                E[(size_t)1 * n + c000] = T(0.25) * (E21_000 + E21_001 + E22_000 + E22_100) +
-                                          T(0.125) * ((dz1214 - dz1234) + (dx1412 - dx3412));
-            }
-            // Ex at (i, j+1/2, k+1/2)
-            {
-                T E11_000 = -fy1_000, E11_001 = -fy1_001;
-                T E12_000 = Fz_bt2[c000], E12_010 = Fz_bt2[c010];
-                T E13_000 = own.ex, E13_010 = y_ex, E13_001 = nxt.ex, E13_011 = yp_ex;
-                T dzL14 = T(2) * (E12_000 - E13_000);
-                T dzR14 = T(2) * (E12_010 - E13_010);
-                T dzL34 = T(2) * (E13_001 - E12_000);
-                T dzR34 = T(2) * (E13_011 - E12_010);
-                T dz1214, dz1234;
-                upwind_pair(vy, dzL14, dzR14, dzL34, dzR34, dz1214, dz1234);
-                T dyL14 = T(2) * (E11_000 - E13_000);
-                T dyR14 = T(2) * (E11_001 - E13_001);
-                T dyL34 = T(2) * (E13_010 - E11_000);
-                T dyR34 = T(2) * (E13_011 - E11_001);
-                T dy1412, dy3412;
-                upwind_pair(vz, dyL14, dyR14, dyL34, dyR34, dy1412, dy3412);
-                E[c000] = T(0.25) * (E11_000 + E11_001 + E12_000 + E12_010) +
-                          T(0.125) * ((dz1214 - dz1234) + (dy1412 - dy3412));
-            }
-            fx2_000 = fx2_001;
-            fy1_000 = fy1_001;
-        }
-        own = nxt;
-        s0 = s1;
-    }
-}
-
 // ============================================================ update
 // update_hydro_state_3d + final_check_unphysical (vanleer_mod.f90:2080-2207,
 // 3243-3262) and update_CT_3d with the cell-centre average (:2211-2259).

@@ -61,21 +61,9 @@ static dim3 grid_of(const BatchDev& b, int kind) {
     }
 }
 
-// Corner EMFs of one stage (PROT: of the protection fluxes): single boxes
-// whose rows are whole 32-cell segments and whose y edge is a multiple of 8
-// take the tiled kernel with shared cell-centre values, the rest the
-// z-column kernel.
+// Corner EMFs of one stage (PROT: of the protection fluxes).
 template <class T, bool ONE, bool PROT>
 static void launch_emf(BatchDev& b, dim3 gz, int half_step_state) {
-    if constexpr (ONE) {
-        const BoxRec& r = b.a.one;
-        if (emf_by_tiles(r.nx, r.ny)) {
-            dim3 g((unsigned)(r.nx / kEmfTX), (unsigned)(r.ny / kEmfTY), (unsigned)((r.nz + kEmfSegZ - 1) / kEmfSegZ));
-            k_corner_emf_tile<T, PROT><<<g, kEmfThreads, 0, b.st>>>(b.a, half_step_state);
-            b.launches += 1;
-            return;
-        }
-    }
     k_corner_emf<T, ONE, PROT><<<gz, kBX, 0, b.st>>>(b.a, half_step_state);
     b.launches += 1;
 }
