@@ -92,6 +92,8 @@ def parse(argv=None):
     ap.add_argument("--served-low", type=int, default=100, help="requests of the sub-saturating stream")
     ap.add_argument("--loop-sample", type=int, default=128,
                     help="boxes of the per-box loop arms, the first of the batch (0: all)")
+    ap.add_argument("--no-loops", action="store_true",
+                    help="skip the per-box loop arms of the batched and served workloads")
     ap.add_argument("--dist-check", action="store_true", help=argparse.SUPPRESS)   # launcher self-test (gloo)
     return ap.parse_args(argv)
 
@@ -530,6 +532,8 @@ def run_batched(a, local, stream, dist, dev):
                     "gpu_launches": bt.launch_count - launches0}
     bt.close()
     del bt
+    if a.no_loops:
+        return out
 
     # plain per-box loops: one Box at a time, the host driver loop over
     # imhd_step; FP64 is the plain method, FP32 the same loop at the batch's
@@ -659,7 +663,7 @@ def run_served(a, local, nreq, rate, loops=True):
            "failed_requests": [{"request": i, "edge": specs[i].n, "riemann": specs[i].riemann,
                                 "mach": round(specs[i].mach, 3), "steps_made": steps_made[i]} for i in failed],
            "server": stats}
-    if not loops:
+    if not loops or a.no_loops:
         return out
     # plain per-box loops over the first requests of the stream, one at a time
     nloop = min(a.loop_sample or len(specs), len(specs), 64)

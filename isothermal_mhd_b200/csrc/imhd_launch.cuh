@@ -171,6 +171,46 @@ static void ensure_passive_tma_attr() {
 // are whole 128-cell tiles (16-byte aligned rows of every field it streams),
 // the z-column kernel otherwise; scalar arrays sized for the table's largest
 // passive count.
+template <class T>
+static void ensure_passive_pred_tma_attr() {
+    static bool attr_set[64] = {};   // per precision and device
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        cudaFuncSetAttribute(k_passive_pred_tma<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)passive_pred_tma_smem_bytes<T, 2>());
+        cudaFuncSetAttribute(k_passive_pred_tma<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)passive_pred_tma_smem_bytes<T, 4>());
+        cudaFuncSetAttribute(k_passive_pred_tma<T, kMaxPass>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)passive_pred_tma_smem_bytes<T, kMaxPass>());
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+}
+
+// Passive predictor: the bulk-copy fed kernel for a single box whose rows are
+// whole 128-cell tiles (16-byte aligned sources), the z-column kernel
+// otherwise; scalar arrays sized for the table's largest passive count.
+template <class T, bool ONE>
+static void launch_passive_pred(BatchDev& b, dim3 gz) {
+    const BoxRec& r = b.a.one;
+    if (ONE && ((uintptr_t)r.S[0] | (uintptr_t)r.SH) % 16 == 0 && passive_by_tma(r.nx)) {
+        ensure_passive_pred_tma_attr<T>();
+        const dim3 g((unsigned)(r.nx / kTmaTile), (unsigned)r.ny, (unsigned)((r.nz + kSegZ - 1) / kSegZ));
+        if (b.npass_max <= 2)
+            k_passive_pred_tma<T, 2><<<g, kTmaTile, passive_pred_tma_smem_bytes<T, 2>(), b.st>>>(b.a);
+        else if (b.npass_max <= 4)
+            k_passive_pred_tma<T, 4><<<g, kTmaTile, passive_pred_tma_smem_bytes<T, 4>(), b.st>>>(b.a);
+        else
+            k_passive_pred_tma<T, kMaxPass><<<g, kTmaTile, passive_pred_tma_smem_bytes<T, kMaxPass>(), b.st>>>(b.a);
+        b.launches += 1;
+        return;
+    }
+    if (b.npass_max <= 2) k_passive_pred<T, ONE, 2><<<gz, kBX, 0, b.st>>>(b.a);
+    else if (b.npass_max <= 4) k_passive_pred<T, ONE, 4><<<gz, kBX, 0, b.st>>>(b.a);
+    else k_passive_pred<T, ONE, kMaxPass><<<gz, kBX, 0, b.st>>>(b.a);
+    b.launches += 1;
+}
+
 template <class T, bool ONE>
 static void launch_passive_corr(BatchDev& b, dim3 gz) {
     const BoxRec& r = b.a.one;
@@ -196,6 +236,7 @@ template <class T>
 cudaError_t prepare_launch(BatchDev& b) {
     ensure_update_tma_attr<T>();
     ensure_passive_tma_attr<T>();
+    ensure_passive_pred_tma_attr<T>();
     for_schemes([&](auto s) {
         if (b.has_scheme[s.value]) {
             ensure_xrow_attr<T, s.value, true>();
@@ -298,11 +339,7 @@ static cudaError_t run_step_t(BatchDev& b, int device_driven) {
     }
     if (b.any_pass) {
         mark(b, kStPassivePred);
-        // scalar arrays sized for the table's largest passive count
-        if (b.npass_max <= 2) k_passive_pred<T, ONE, 2><<<gz, kBX, 0, b.st>>>(b.a);
-        else if (b.npass_max <= 4) k_passive_pred<T, ONE, 4><<<gz, kBX, 0, b.st>>>(b.a);
-        else k_passive_pred<T, ONE, kMaxPass><<<gz, kBX, 0, b.st>>>(b.a);
-        b.launches += 1;
+        launch_passive_pred<T, ONE>(b, gz);
         mark(b, kStPassiveCorr);
         launch_passive_corr<T, ONE>(b, gz);
     }
