@@ -669,8 +669,13 @@ __device__ __forceinline__ CellEV<T> cell_ev(const T* __restrict__ S, int n, int
 // PROT: the corner EMFs of the protection fluxes (Fp -> Ep) of the boxes
 // that compute them, the second compute_cell_corner_emf_3d call of
 // vanleer_mod.f90:336, 396 (the cell-centre EMFs are the same).
+// FP32 occupancy: six blocks per SM for a single box (eight spilled more than
+// they gained, 2.2 -> 2.4 ms at 512^3); eight in a table, whose small boxes
+// leave the loads less overlapped (the batched workload 4.48 -> 4.70e9
+// cell-updates/s).
 template <class T, bool ONE, bool PROT = false>
-__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? 6 : 1) k_corner_emf(BatchArgs ba, int half_step_state) {
+__global__ void __launch_bounds__(kBX, sizeof(T) == 4 ? (ONE ? 6 : 8) : 1) k_corner_emf(BatchArgs ba,
+                                                                                       int half_step_state) {
     int local;
     const BoxRec rp = resolve<ONE>(ba, kKindCellZ, local);
     if (!rp.active || (PROT && !rp.protect)) return;
