@@ -39,9 +39,10 @@ def test_fp64_noncubic_bit_exact(n, riemann, recon):
 
 
 @pytest.mark.parametrize("n,npass", [((32, 16, 36), 0), ((32, 16, 36), 2), ((32, 16, 36), 3), ((32, 16, 36), 5),
-                                     ((128, 12, 20), 3), ((128, 12, 20), 5)])
+                                     ((128, 12, 20), 3), ((128, 12, 20), 5), ((128, 13, 16), 2)])
 def test_fp64_passive_counts(n, npass):
-    # 128-cell rows: the bulk-copy fed passive kernels with scalar arrays sized 4 and 8
+    # 128-cell rows: the bulk-copy fed passive kernels with scalar arrays sized 4 and 8; an odd
+    # row count: the corrector's blocks of one row instead of two
     q, b, p = problems.smooth_wave_box(n, npass=1)
     rng = np.random.default_rng(11)
     p = rng.uniform(0.0, 1.0, (npass,) + q.shape[1:])
