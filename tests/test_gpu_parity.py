@@ -289,7 +289,7 @@ def test_non_finite_state_returns_physics_error(precision):
 
 @pytest.mark.parametrize("ic_kind,riemann", [("smooth", "roe"), ("turbulent", "roe"), ("turbulent", "hlld")])
 def test_fp32_64cubed_100_steps_within_1e5_of_fp64(ic_kind, riemann):
-    # the north-star accuracy bound at a size the test run affords: 64^3, 100
+    # the FP32 accuracy bound (1e-5 after 100 steps) at a size the test run affords: 64^3, 100
     # steps, relative L1 <= 1e-5 per field of the FP32 step against the FP64
     # GPU path (itself bit-exact with the oracle at 64^3 x 100 steps, see
     # test_gpu_golden), on the FP64 run's dt sequence.  "turbulent": rms Mach 2
