@@ -525,11 +525,13 @@ __global__ void __launch_bounds__(TX) k_corr_flux_x(BatchArgs ba) {
 // exactly once (the tiled kernel above recomputes slopes at tile edges and
 // stages a halo).  PPM evaluates the edges of cells i and i+1 per face.
 // Needs 13 * nx * sizeof(T) bytes of dynamic shared memory.
-// FP32: 64 registers; eight 128-thread blocks per SM (smaller barrier
-// groups, 27 KB of shared memory each at nx = 512): 3.45 -> 3.19 ms (Roe,
-// PLM) at 512^3 against four 256-thread blocks.
+// FP32: 128-thread blocks (smaller barrier groups, 27 KB of shared memory
+// each at nx = 512): 3.45 -> 3.22 ms (Roe, PLM) at 512^3 against four
+// 256-thread blocks.  A single box runs six per SM at 80 registers without
+// spills (3.22 -> 3.19 ms); a table keeps eight at 64 (six: batched workload
+// 4.67 -> 4.58e9 cell-updates/s).
 template <class T, int SCHEME, bool ONE>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 8 : 1) k_corr_flux_xrow(BatchArgs ba) {
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (ONE ? 6 : 8) : 1) k_corr_flux_xrow(BatchArgs ba) {
     constexpr int SOLVER = scheme_solver(SCHEME);
     constexpr int RECON = scheme_recon(SCHEME);
     constexpr bool PPM = (RECON & 1) != 0, PRIM = (RECON & 2) != 0;
